@@ -1,0 +1,922 @@
+// bc_gpu.cu — host side of libbcgpu: planning, tables, device arena, class
+// batching, launches, rounding-error checks with narrower-width retry, and
+// the C ABI declared in include/bc_gpu.h.
+//
+// The reference multiply (_fft_mul, bigfloat/mul.c:108-174) picks a width
+// from CL alone (mul.c:109-124), allocates two arrays per call (mul.c:133-138)
+// and aborts on widths it has no packer for (fft/convert.c:66-68).  Here the
+// width is the narrowest one that fits the smallest transform allowed by the
+// width table, scratch comes from one device arena, and every failure is a
+// status code.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bc_gpu.h"
+#include "bc_kernels.cuh"
+
+using namespace bc;
+
+namespace {
+
+// ------------------------------------------------------------------ shapes
+struct Shape {
+  int M = 0, L1 = 0, L2 = 1, Lr = 1, levels = 0;
+};
+
+constexpr int kRowLens[] = {128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096};
+constexpr int kSmallLens[] = {256, 512, 768, 1024, 1536, 2048, 3072, 4096};
+constexpr int kOuterLens[] = {64, 128, 256, 512};
+constexpr size_t kMaxM = size_t(1) << 30;
+
+bool is_row_len(size_t L) {
+  for (int x : kRowLens) if ((size_t)x == L) return true;
+  return false;
+}
+size_t pow2part(size_t x) { return x & (~x + 1); }
+
+bool shape_for(size_t M, Shape &s) {
+  if (M < 256 || M > kMaxM) return false;
+  const size_t p2 = (M % 3 == 0) ? M / 3 : M;
+  if (p2 & (p2 - 1)) return false;
+  if (M <= 4096) {
+    for (int x : kSmallLens)
+      if ((size_t)x == M) { s.M = (int)M; s.L1 = (int)M; s.L2 = 1; s.Lr = 1; s.levels = 1; return true; }
+    return false;
+  }
+  for (int L1 : kOuterLens) {
+    if (M % L1) continue;
+    const size_t Lr = M / L1;
+    if (is_row_len(Lr) && pow2part(Lr) >= (size_t)(4096 / L1)) {
+      s.M = (int)M; s.L1 = L1; s.L2 = 1; s.Lr = (int)Lr; s.levels = 2; return true;
+    }
+  }
+  for (int i = (int)(sizeof(kRowLens) / sizeof(int)) - 1; i >= 0; i--) {
+    const size_t Lr = kRowLens[i];
+    if (Lr < 512 || M % Lr) continue;
+    const size_t R = M / Lr;
+    for (int L1 : kOuterLens) {
+      if (R % L1) continue;
+      const size_t L2 = R / L1;
+      if (L2 < 64 || L2 > 512 || (L2 & (L2 - 1)) || L2 > (size_t)L1) continue;
+      if (pow2part(Lr) < 4096 / L2) continue;
+      s.M = (int)M; s.L1 = L1; s.L2 = (int)L2; s.Lr = (int)Lr; s.levels = 3; return true;
+    }
+  }
+  return false;
+}
+
+// Transform lengths in increasing order: 2^k and 3*2^k with a valid shape.
+const std::vector<size_t> &lengths() {
+  static std::vector<size_t> v = [] {
+    std::vector<size_t> r;
+    for (size_t p = 256; p <= kMaxM; p *= 2) {
+      Shape s;
+      if (shape_for(p, s)) r.push_back(p);
+      if (3 * p / 2 <= kMaxM && shape_for(3 * p / 2, s)) r.push_back(3 * p / 2);
+    }
+    std::sort(r.begin(), r.end());
+    return r;
+  }();
+  return v;
+}
+
+// ------------------------------------------------------------------ state
+struct Tables {
+  double2 *dev = nullptr;
+  const double2 *twL1 = nullptr, *twL2 = nullptr, *twLr = nullptr, *pw_fwd = nullptr, *pw_inv = nullptr;
+  Tw2 tw4M{};
+};
+
+struct Ctx {
+  bool init = false;
+  int device = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  char *arena = nullptr;
+  size_t arena_cap = 0, arena_limit = 0;
+  std::map<size_t, Tables> tables;
+  std::map<size_t, int> width_override;
+  std::map<size_t, int> width_file;
+  int forced_width = 0;
+  double max_err = 0.25;
+  int verbose = 0;
+  int last_error = 0;
+  int last_cuda = 0;
+  bool time_kernels = false;
+  std::vector<std::pair<const char *, double>> ktimes;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> kev;
+  int sm_count = 148;
+};
+
+Ctx g;
+std::recursive_mutex g_mu;
+
+int fail(int code) {
+  g.last_error = code;
+  return code;
+}
+
+#define CK(call)                                                                 \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess) {                                                     \
+      g.last_cuda = (int)e_;                                                     \
+      if (g.verbose) fprintf(stderr, "bc_gpu: %s failed: %s (%s:%d)\n", #call,   \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);        \
+      return fail(e_ == cudaErrorMemoryAllocation ? BC_ERR_NOMEM : BC_ERR_CUDA); \
+    }                                                                            \
+  } while (0)
+
+// ------------------------------------------------------------------ widths
+// Default width limit at transform length M: about 2b + log2(M)/2 stays near
+// the FP64 budget for a max rounding error below 0.25 on random digits.
+// Replaced per length by the tuned table (bc_tune file) when present.
+int default_width_limit(size_t M) {
+  const double lg = std::log2((double)M);
+  int b = (int)std::floor(23.0 - 0.3 * lg);
+  return std::max(8, std::min(24, b));
+}
+
+int width_limit(size_t M) {
+  auto it = g.width_override.find(M);
+  if (it != g.width_override.end()) return it->second;
+  it = g.width_file.find(M);
+  if (it != g.width_file.end()) return it->second;
+  return default_width_limit(M);
+}
+
+void load_width_file(const char *path) {
+  if (!path) path = getenv("BC_TUNE_FILE");
+  std::string p;
+  if (path) p = path;
+  if (p.empty()) return;
+  FILE *f = fopen(p.c_str(), "r");
+  if (!f) return;
+  char line[256];
+  while (fgets(line, sizeof line, f)) {
+    if (line[0] == '#') continue;
+    unsigned long long M = 0;
+    int b = 0;
+    if (sscanf(line, "%llu %d", &M, &b) == 2 && b >= 8 && b <= 24) g.width_file[(size_t)M] = b;
+  }
+  fclose(f);
+}
+
+// ------------------------------------------------------------------ plans
+struct Plan {
+  Shape shape;
+  int b = 0;
+  size_t AL = 0, BL = 0;     // clamped to CL
+  size_t ndA = 0, ndB = 0;
+  size_t nwords = 0, nruns = 0, ntiles = 0;
+  bool square = false;
+};
+
+size_t ndigits(size_t XL, int b) { return (32 * (uint64_t)XL + b - 1) / b; }
+
+// HBM passes over the complex data per product, relative to two levels: the
+// 3-level shape adds a read+write of every operand and of the product.
+double shape_cost(const Shape &s) { return (double)s.M * (s.levels == 3 ? 2.0 : 1.0); }
+
+bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl) {
+  pl = Plan();
+  pl.AL = std::min(AL, CL);
+  pl.BL = std::min(BL, CL);
+  pl.square = square;
+  bool found = false;
+  double best = 0;
+  size_t first_fit = 0;
+  for (size_t M : lengths()) {
+    if (first_fit && M > 4 * first_fit) break;
+    int bmax = std::min(width_limit(M), bcap);
+    if (g.forced_width) bmax = g.forced_width;
+    if (bmax < 8) continue;
+    auto fits = [&](int b) {
+      const size_t na = ndigits(pl.AL, b), nb = ndigits(pl.BL, b);
+      return na + nb <= 2 * M + 1;
+    };
+    if (!fits(bmax)) continue;
+    if (!first_fit) first_fit = M;
+    Shape s;
+    shape_for(M, s);
+    const double cost = shape_cost(s);
+    if (found && cost >= best) continue;
+    int b = bmax;
+    if (!g.forced_width)
+      while (b > 8 && fits(b - 1)) b--;
+    found = true;
+    best = cost;
+    pl.shape = s;
+    pl.b = b;
+  }
+  if (!found) return false;
+  const size_t M = pl.shape.M;
+  const int b = pl.b;
+  pl.ndA = ndigits(pl.AL, b);
+  pl.ndB = ndigits(pl.BL, b);
+  const size_t prod_words = (2 * M * (uint64_t)b) / 32;
+  pl.nwords = std::min(CL, prod_words);
+  pl.nruns = std::min((size_t)(2 * M / 8), (pl.nwords * 32 + 8 * b - 1) / (8 * b));
+  pl.ntiles = std::max<size_t>(1, (pl.nruns + CARRY_NT - 1) / CARRY_NT);
+  return true;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+size_t work_bytes(const Plan &pl) {
+  const size_t M = pl.shape.M;
+  size_t w = align256(M * 16);                           // bufA
+  if (!pl.square) w += align256(M * 16);                 // bufB
+  if (pl.shape.levels > 1) w += align256(M / 4 * sizeof(RunRec)) + align256(pl.ntiles * 4);  // run records + status
+  return w;
+}
+
+// ------------------------------------------------------------------ tables
+double2 cis_neg(long double num, long double den, long double scale) {
+  // e^{-2 pi i num/den} * scale, evaluated in long double
+  long double a = 2.0L * 3.141592653589793238462643383279502884L * (num / den);
+  return make_double2((double)(cosl(a) * scale), (double)(-sinl(a) * scale));
+}
+
+int ensure_tables(const Shape &s, Tables **out) {
+  auto it = g.tables.find((size_t)s.M);
+  if (it != g.tables.end()) { *out = &it->second; return BC_OK; }
+  const size_t M = s.M;
+  const size_t four = 4 * M;
+  int h = 0;
+  while ((size_t(1) << (2 * h)) < four) h++;
+  const size_t nlo = size_t(1) << h, nhi = (four + nlo - 1) / nlo;
+  const bool small = s.levels == 1;
+  const size_t nL2 = s.levels == 3 ? s.L2 : 0, nLr = s.levels >= 2 ? s.Lr : 0;
+  const size_t total = s.L1 + nL2 + nLr + 2 * (size_t)s.L1 + (small ? 0 : nlo + nhi);
+  std::vector<double2> host(total);
+  size_t o = 0;
+  auto block = [&](size_t L) {
+    for (size_t m = 0; m < L; m++) host[o + m] = cis_neg((long double)m, (long double)L, 1.0L);
+    size_t at = o;
+    o += L;
+    return at;
+  };
+  const size_t oL1 = block(s.L1);
+  const size_t oL2 = nL2 ? block(nL2) : 0;
+  const size_t oLr = nLr ? block(nLr) : 0;
+  const size_t opf = o;
+  for (size_t n = 0; n < (size_t)s.L1; n++) {
+    // e^{+i pi n/(2 L1)} = conj(e^{-2 pi i n/(4 L1)})
+    double2 w = cis_neg((long double)n, 4.0L * s.L1, 1.0L);
+    host[o + n] = make_double2(w.x, -w.y);
+  }
+  o += s.L1;
+  const size_t opi = o;
+  for (size_t n = 0; n < (size_t)s.L1; n++) host[o + n] = cis_neg((long double)n, 4.0L * s.L1, 1.0L / (long double)M);
+  o += s.L1;
+  size_t olo = 0, ohi = 0;
+  if (!small) {
+    olo = o;
+    for (size_t m = 0; m < nlo; m++) host[o + m] = cis_neg((long double)m, (long double)four, 1.0L);
+    o += nlo;
+    ohi = o;
+    for (size_t m = 0; m < nhi; m++) host[o + m] = cis_neg((long double)(m * nlo), (long double)four, 1.0L);
+    o += nhi;
+  }
+  Tables t;
+  CK(cudaMalloc(&t.dev, total * sizeof(double2)));
+  CK(cudaMemcpy(t.dev, host.data(), total * sizeof(double2), cudaMemcpyHostToDevice));
+  t.twL1 = t.dev + oL1;
+  t.twL2 = nL2 ? t.dev + oL2 : nullptr;
+  t.twLr = nLr ? t.dev + oLr : nullptr;
+  t.pw_fwd = t.dev + opf;
+  t.pw_inv = t.dev + opi;
+  if (!small) {
+    t.tw4M.lo = t.dev + olo;
+    t.tw4M.hi = t.dev + ohi;
+    t.tw4M.mask = nlo - 1;
+    t.tw4M.h = h;
+  }
+  auto res = g.tables.emplace(M, t);
+  *out = &res.first->second;
+  return BC_OK;
+}
+
+// ------------------------------------------------------------------ kernels
+typedef void (*KFn)(ClassParams);
+
+template <int L> constexpr int rows_per_cta() {
+  constexpr int tc = L / PTS;
+  return tc >= 256 ? 1 : (256 / tc >= 16 ? 16 : (256 / tc >= 8 ? 8 : (256 / tc >= 4 ? 4 : (256 / tc >= 2 ? 2 : 1))));
+}
+
+struct KInfo {
+  KFn fn = nullptr;
+  int threads = 0;
+  size_t smem = 0;
+  const char *name = "";
+};
+
+template <int L, int W>
+KInfo outer_fwd_info() {
+  return {k_outer_fwd<L, W>, (L / PTS) * W, TileSmem<L, W>::elems * sizeof(double2), "outer_fwd"};
+}
+template <int L, int W>
+KInfo outer_inv_info() {
+  return {k_outer_inv<L, W>, (L / PTS) * W, TileSmem<L, W>::elems * sizeof(double2), "outer_inv"};
+}
+template <int L, bool INV>
+KInfo mid_info() {
+  constexpr int W = 4096 / L;
+  return {k_mid<L, W, INV>, (L / PTS) * W, TileSmem<L, W>::elems * sizeof(double2), INV ? "mid_inv" : "mid_fwd"};
+}
+template <int L, bool SQ>
+KInfo rows_info() {
+  constexpr int NR = rows_per_cta<L>();
+  return {k_rows<L, NR, SQ>, (L / PTS) * NR, (size_t)NR * TileSmem<L, 1>::elems * sizeof(double2), "rows"};
+}
+template <int M, bool SQ>
+KInfo small_info() {
+  return {k_small<M, SQ>, M / PTS, TileSmem<M, 1>::elems * sizeof(double2), "small"};
+}
+
+KInfo get_outer(int L, bool inv) {
+  switch (L) {
+    case 64: return inv ? outer_inv_info<64, 64>() : outer_fwd_info<64, 64>();
+    case 128: return inv ? outer_inv_info<128, 32>() : outer_fwd_info<128, 32>();
+    case 256: return inv ? outer_inv_info<256, 16>() : outer_fwd_info<256, 16>();
+    case 512: return inv ? outer_inv_info<512, 8>() : outer_fwd_info<512, 8>();
+  }
+  return {};
+}
+KInfo get_mid(int L, bool inv) {
+  switch (L) {
+    case 64: return inv ? mid_info<64, true>() : mid_info<64, false>();
+    case 128: return inv ? mid_info<128, true>() : mid_info<128, false>();
+    case 256: return inv ? mid_info<256, true>() : mid_info<256, false>();
+    case 512: return inv ? mid_info<512, true>() : mid_info<512, false>();
+  }
+  return {};
+}
+#define ROWCASE(L) \
+  case L: return sq ? rows_info<L, true>() : rows_info<L, false>();
+KInfo get_rows(int L, bool sq) {
+  switch (L) {
+    ROWCASE(128) ROWCASE(192) ROWCASE(256) ROWCASE(384) ROWCASE(512) ROWCASE(768)
+    ROWCASE(1024) ROWCASE(1536) ROWCASE(2048) ROWCASE(3072) ROWCASE(4096)
+  }
+  return {};
+}
+#define SMALLCASE(L) \
+  case L: return sq ? small_info<L, true>() : small_info<L, false>();
+KInfo get_small(int M, bool sq) {
+  switch (M) {
+    SMALLCASE(256) SMALLCASE(512) SMALLCASE(768) SMALLCASE(1024) SMALLCASE(1536) SMALLCASE(2048)
+    SMALLCASE(3072) SMALLCASE(4096)
+  }
+  return {};
+}
+
+std::map<KFn, int> g_occ;  // resident CTAs per SM, per kernel
+
+int prepare(const KInfo &k, int *grid_cap) {
+  auto it = g_occ.find(k.fn);
+  if (it == g_occ.end()) {
+    if (k.smem > 48 * 1024) CK(cudaFuncSetAttribute((const void *)k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+    int n = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void *)k.fn, k.threads, k.smem));
+    if (n < 1) n = 1;
+    it = g_occ.emplace(k.fn, n).first;
+  }
+  *grid_cap = it->second * g.sm_count;
+  return BC_OK;
+}
+
+int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunch) {
+  int cap = 0;
+  int r = prepare(k, &cap);
+  if (r) return r;
+  const int grid = (int)std::max<long long>(1, std::min<long long>(units, cap));
+  k.fn<<<grid, k.threads, k.smem, g.stream>>>(p);
+  CK(cudaGetLastError());
+  (*nlaunch)++;
+  if (g.time_kernels) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, g.stream));
+    g.kev.push_back(e);
+    g.ktimes.push_back({k.name, 0.0});
+  }
+  return BC_OK;
+}
+
+// ------------------------------------------------------------------ arena
+int arena_reserve(size_t bytes) {
+  if (bytes <= g.arena_cap) return BC_OK;
+  if (bytes > g.arena_limit) return fail(BC_ERR_NOMEM);
+  if (g.arena) {
+    CK(cudaStreamSynchronize(g.stream));
+    CK(cudaFree(g.arena));
+    g.arena = nullptr;
+    g.arena_cap = 0;
+  }
+  size_t want = std::min(g.arena_limit, std::max(bytes + bytes / 4, (size_t)64 << 20));
+  cudaError_t e = cudaMalloc(&g.arena, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    want = bytes;
+    e = cudaMalloc(&g.arena, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      g.arena = nullptr;
+      return fail(BC_ERR_NOMEM);
+    }
+  }
+  g.arena_cap = want;
+  return BC_OK;
+}
+
+bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// ------------------------------------------------------------------ batch core
+struct Work {
+  size_t idx;      // index into the caller's items
+  Plan pl;
+  int bcap;
+  int retries = 0;
+  double err = 0;
+  unsigned flags = 0;
+  bool done = false;
+};
+
+struct Run {
+  // per item device pointers (inside the arena)
+  const uint32_t *dA = nullptr, *dB = nullptr;
+  uint32_t *dC = nullptr;
+  bool hostC = false;    // destination is host memory (copied out after the check)
+  bool stagedC = false;  // device destination overlaps an input: computed in scratch
+};
+
+bool overlaps(const void *a, size_t abytes, const void *b, size_t bbytes) {
+  const char *x = (const char *)a, *y = (const char *)b;
+  return abytes && bbytes && x < y + bbytes && y < x + abytes;
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Run one attempt over `works` (all not done).  Fills err/flags.
+int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st) {
+  // ---- memory layout
+  struct Slot { size_t off_dA, off_dB, off_dC, off_work, off_desc; };
+  std::vector<Slot> slots(works.size());
+  size_t off = 0;
+  std::vector<Run> runs(works.size());
+  std::vector<char> hostA(works.size()), hostB(works.size());
+  for (size_t i = 0; i < works.size(); i++) {
+    const bc_mul_desc &d = items[works[i]->idx];
+    const Plan &pl = works[i]->pl;
+    hostA[i] = pl.AL && !is_device_ptr(d.A);
+    hostB[i] = !pl.square && pl.BL && !is_device_ptr(d.B);
+    runs[i].hostC = !is_device_ptr(d.C);
+    runs[i].stagedC = !runs[i].hostC && (overlaps(d.C, d.CL * 4, d.A, d.AL * 4) || overlaps(d.C, d.CL * 4, d.B, d.BL * 4));
+    slots[i].off_dA = off; if (hostA[i]) off += align256(pl.AL * 4);
+    slots[i].off_dB = off; if (hostB[i]) off += align256(pl.BL * 4);
+    slots[i].off_dC = off; if (runs[i].hostC || runs[i].stagedC) off += align256(d.CL * 4);
+    slots[i].off_work = off; off += work_bytes(pl);
+  }
+  const size_t off_err = off; off += align256(works.size() * 8);
+  const size_t off_flags = off; off += align256(works.size() * 4);
+  const size_t off_desc = off; off += align256(works.size() * sizeof(ItemDesc));
+  const size_t off_ctr = off; off += 256 * (works.size() + 1);
+  int r = arena_reserve(off);
+  if (r) return r;
+  char *base = g.arena;
+
+  auto t_h2d = std::chrono::steady_clock::now();
+  // ---- inputs
+  for (size_t i = 0; i < works.size(); i++) {
+    const bc_mul_desc &d = items[works[i]->idx];
+    const Plan &pl = works[i]->pl;
+    runs[i].dA = hostA[i] ? (const uint32_t *)(base + slots[i].off_dA) : d.A;
+    if (hostA[i]) {
+      CK(cudaMemcpyAsync((void *)runs[i].dA, d.A, pl.AL * 4, cudaMemcpyHostToDevice, g.stream));
+      st->h2d_bytes += pl.AL * 4;
+    }
+    if (pl.square) runs[i].dB = runs[i].dA;
+    else {
+      runs[i].dB = hostB[i] ? (const uint32_t *)(base + slots[i].off_dB) : d.B;
+      if (hostB[i]) {
+        CK(cudaMemcpyAsync((void *)runs[i].dB, d.B, pl.BL * 4, cudaMemcpyHostToDevice, g.stream));
+        st->h2d_bytes += pl.BL * 4;
+      }
+    }
+    runs[i].dC = (runs[i].hostC || runs[i].stagedC) ? (uint32_t *)(base + slots[i].off_dC) : d.C;
+  }
+  CK(cudaMemsetAsync(base + off_err, 0, off_desc - off_err, g.stream));
+
+  // ---- descriptors, grouped by class (M, square)
+  std::map<std::pair<size_t, bool>, std::vector<size_t>> classes;
+  for (size_t i = 0; i < works.size(); i++) classes[{(size_t)works[i]->pl.shape.M, works[i]->pl.square}].push_back(i);
+  std::vector<ItemDesc> desc(works.size());
+  std::vector<size_t> order;
+  order.reserve(works.size());
+  for (auto &c : classes) {
+    unsigned long long tile0 = 0;
+    for (size_t i : c.second) {
+      const bc_mul_desc &d = items[works[i]->idx];
+      const Plan &pl = works[i]->pl;
+      ItemDesc &it = desc[order.size()];
+      order.push_back(i);
+      char *w = base + slots[i].off_work;
+      const size_t M = pl.shape.M;
+      it.A = runs[i].dA;
+      it.B = runs[i].dB;
+      it.C = runs[i].dC;
+      it.AL = pl.AL; it.BL = pl.BL; it.CL = d.CL;
+      it.ndA = pl.ndA; it.ndB = pl.square ? pl.ndA : pl.ndB;
+      it.bufA = (double2 *)w; w += align256(M * 16);
+      it.bufB = nullptr;
+      if (!pl.square) { it.bufB = (double2 *)w; w += align256(M * 16); }
+      it.rec = nullptr; it.status = nullptr;
+      if (pl.shape.levels > 1) {
+        it.rec = (RunRec *)w; w += align256(M / 4 * sizeof(RunRec));
+        it.status = (uint32_t *)w; w += align256(pl.ntiles * 4);
+      }
+      it.nwords = pl.nwords;
+      it.nruns = pl.nruns;
+      it.tile0 = tile0;
+      tile0 += pl.ntiles;
+      it.err = (unsigned long long *)(base + off_err) + i;
+      it.flags = (unsigned int *)(base + off_flags) + i;
+      it.b = pl.b;
+      it.square = pl.square ? 1 : 0;
+    }
+  }
+  // status words must start at zero for every attempt
+  for (size_t k = 0; k < order.size(); k++) {
+    const ItemDesc &it = desc[k];
+    if (it.status) CK(cudaMemsetAsync(it.status, 0, works[order[k]]->pl.ntiles * 4, g.stream));
+  }
+  ItemDesc *ddesc = (ItemDesc *)(base + off_desc);
+  CK(cudaMemcpyAsync(ddesc, desc.data(), desc.size() * sizeof(ItemDesc), cudaMemcpyHostToDevice, g.stream));
+  unsigned int *ctr = (unsigned int *)(base + off_ctr);
+  CK(cudaMemsetAsync(ctr, 0, 256 * (works.size() + 1), g.stream));
+  const double h2d_ms = ms_since(t_h2d);
+  (void)h2d_ms;
+
+  // ---- launches
+  CK(cudaEventRecord(g.ev0, g.stream));
+  size_t first = 0, cls = 0;
+  for (auto &c : classes) {
+    const size_t n = c.second.size();
+    const Plan &pl = works[c.second[0]]->pl;
+    const Shape &s = pl.shape;
+    const bool sq = c.first.second;
+    Tables *tb = nullptr;
+    r = ensure_tables(s, &tb);
+    if (r) return r;
+    ClassParams p{};
+    p.M = s.M; p.L1 = s.L1; p.S1 = s.M / s.L1; p.L2 = s.L2; p.Lr = s.levels == 3 ? s.Lr : p.S1;
+    p.tw4M = tb->tw4M; p.pw_fwd = tb->pw_fwd; p.pw_inv = tb->pw_inv;
+    p.twL1 = tb->twL1; p.twL2 = tb->twL2; p.twLr = tb->twLr;
+    p.items = ddesc + first;
+    p.nitems = (int)n;
+    p.counter = ctr + 64 * cls;
+    unsigned long long tiles = 0;
+    for (size_t k = first; k < first + n; k++) tiles += works[order[k]]->pl.ntiles;
+    p.carry_tiles = tiles;
+    size_t &nl = st->launches;
+    if (s.levels == 1) {
+      r = launch(get_small(s.M, sq), (long long)n, p, &nl);
+      if (r) return r;
+    } else {
+      const long long S1 = p.S1;
+      KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
+      const int W1 = ko.threads / (s.L1 / PTS);
+      if ((r = launch(ko, (long long)n * 2 * (S1 / W1), p, &nl))) return r;
+      if (s.levels == 3) {
+        KInfo km = get_mid(s.L2, false);
+        const int W2 = km.threads / (s.L2 / PTS);
+        if ((r = launch(km, (long long)n * 2 * s.L1 * (s.Lr / W2), p, &nl))) return r;
+      }
+      KInfo kr = get_rows(s.Lr, sq);
+      const int NR = kr.threads / (s.Lr / PTS);
+      if ((r = launch(kr, (long long)n * (s.M / s.Lr / NR), p, &nl))) return r;
+      if (s.levels == 3) {
+        KInfo km = get_mid(s.L2, true);
+        const int W2 = km.threads / (s.L2 / PTS);
+        if ((r = launch(km, (long long)n * s.L1 * (s.Lr / W2), p, &nl))) return r;
+      }
+      if ((r = launch(ki, (long long)n * (S1 / W1), p, &nl))) return r;
+      KInfo kc{k_carry, CARRY_NT, 0, "carry"};
+      if ((r = launch(kc, (long long)tiles, p, &nl))) return r;
+    }
+    first += n;
+    cls++;
+  }
+  CK(cudaEventRecord(g.ev1, g.stream));
+  st->classes += classes.size();
+
+  // ---- verdicts, then outputs of the products that passed
+  std::vector<unsigned long long> errs(works.size());
+  std::vector<unsigned> flags(works.size());
+  CK(cudaMemcpyAsync(errs.data(), base + off_err, works.size() * 8, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaMemcpyAsync(flags.data(), base + off_flags, works.size() * 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, g.ev0, g.ev1));
+  st->device_ms += ms;
+  if (g.time_kernels && !g.kev.empty()) {
+    cudaEvent_t prev = g.ev0;
+    for (size_t k = 0; k < g.kev.size(); k++) {
+      float km = 0;
+      cudaEventElapsedTime(&km, prev, g.kev[k]);
+      g.ktimes[g.ktimes.size() - g.kev.size() + k].second = km;
+      prev = g.kev[k];
+    }
+    for (auto e : g.kev) cudaEventDestroy(e);
+    g.kev.clear();
+  }
+  bool copies = false;
+  for (size_t i = 0; i < works.size(); i++) {
+    double e;
+    memcpy(&e, &errs[i], 8);
+    works[i]->err = e;
+    works[i]->flags = flags[i];
+    const bool ok = ((e < g.max_err) && !(flags[i] & FLAG_TOPCARRY)) || g.forced_width;
+    const bc_mul_desc &d = items[works[i]->idx];
+    if (!ok || flags[i] & FLAG_TIMEOUT) continue;
+    if (runs[i].hostC) {
+      CK(cudaMemcpyAsync(d.C, runs[i].dC, d.CL * 4, cudaMemcpyDeviceToHost, g.stream));
+      st->d2h_bytes += d.CL * 4;
+      copies = true;
+    } else if (runs[i].stagedC) {
+      CK(cudaMemcpyAsync(d.C, runs[i].dC, d.CL * 4, cudaMemcpyDeviceToDevice, g.stream));
+      copies = true;
+    }
+  }
+  if (copies) CK(cudaStreamSynchronize(g.stream));
+  return BC_OK;
+}
+
+int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Plan *first_plan = nullptr) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (n && !items) return fail(BC_ERR_INVALID);
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<Work> works;
+  works.reserve(n);
+  for (size_t i = 0; i < n; i++) {
+    const bc_mul_desc &d = items[i];
+    if (d.CL && !d.C) return fail(BC_ERR_INVALID);
+    if ((d.AL && !d.A) || (d.BL && !d.B)) return fail(BC_ERR_INVALID);
+    if (d.CL == 0) continue;
+    const bool zero = d.AL == 0 || d.BL == 0;
+    if (zero) {
+      if (is_device_ptr(d.C)) CK(cudaMemsetAsync(d.C, 0, d.CL * 4, g.stream));
+      else memset(d.C, 0, d.CL * 4);
+      continue;
+    }
+    Work w;
+    w.idx = i;
+    w.bcap = 24;
+    const bool square = d.A == d.B && d.AL == d.BL;
+    if (!make_plan(d.AL, d.BL, d.CL, square, w.bcap, w.pl)) return fail(BC_ERR_TOO_LARGE);
+    works.push_back(w);
+  }
+  st->items = n;
+  if (g.time_kernels) g.ktimes.clear();
+  // attempts: redo items whose rounding error reached the limit at a narrower width
+  for (int attempt = 0; attempt < 12; attempt++) {
+    std::vector<Work *> todo;
+    for (auto &w : works) if (!w.done) todo.push_back(&w);
+    if (todo.empty()) break;
+    // split into chunks that fit the arena limit
+    size_t i0 = 0;
+    while (i0 < todo.size()) {
+      size_t bytes = 0, i1 = i0;
+      while (i1 < todo.size()) {
+        const bc_mul_desc &d = items[todo[i1]->idx];
+        size_t need = work_bytes(todo[i1]->pl) + align256(d.AL * 4) + align256(d.BL * 4) + align256(d.CL * 4) + 1024;
+        if (i1 > i0 && bytes + need > g.arena_limit / 2) break;
+        bytes += need;
+        i1++;
+      }
+      std::vector<Work *> chunk(todo.begin() + i0, todo.begin() + i1);
+      int r = run_attempt(items, chunk, st);
+      if (r) return r;
+      i0 = i1;
+    }
+    for (Work *w : todo) {
+      if (w->flags & FLAG_TIMEOUT) return fail(BC_ERR_TIMEOUT);
+      st->max_round_err = std::max(st->max_round_err, w->err);
+      const bool bad = !(w->err < g.max_err) || (w->flags & FLAG_TOPCARRY);
+      if (!bad || g.forced_width) {
+        if (w->flags & FLAG_TOPCARRY) return fail(BC_ERR_CARRY);
+        w->done = true;
+        continue;
+      }
+      // narrower digits (and a longer transform if needed)
+      const bc_mul_desc &d = items[w->idx];
+      w->bcap = w->pl.b - 1;
+      w->retries++;
+      st->retries++;
+      if (g.verbose)
+        fprintf(stderr, "bc_gpu: item %zu M=%d b=%d err=%.3g flags=%u -> retry at b<=%d\n", w->idx,
+                w->pl.shape.M, w->pl.b, w->err, w->flags, w->bcap);
+      if (w->bcap < 8 || !make_plan(d.AL, d.BL, d.CL, w->pl.square, w->bcap, w->pl)) return fail(BC_ERR_PRECISION);
+    }
+  }
+  for (auto &w : works)
+    if (!w.done) return fail(BC_ERR_PRECISION);
+  if (first_plan && !works.empty()) *first_plan = works[0].pl;
+  st->total_ms += ms_since(t0);
+  return BC_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int bc_gpu_init(const bc_gpu_config *cfg) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (g.init) return BC_OK;
+  bc_gpu_config c{};
+  if (cfg) c = *cfg;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(BC_ERR_NO_DEVICE);
+  }
+  if (c.device < 0 || c.device >= ndev) return fail(BC_ERR_INVALID);
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, c.device));
+  if (prop.major != 10) return fail(BC_ERR_NO_DEVICE);
+  CK(cudaSetDevice(c.device));
+  g.device = c.device;
+  g.sm_count = prop.multiProcessorCount;
+  CK(cudaStreamCreateWithFlags(&g.own_stream, cudaStreamNonBlocking));
+  g.stream = g.own_stream;
+  CK(cudaEventCreate(&g.ev0));
+  CK(cudaEventCreate(&g.ev1));
+  size_t fre = 0, tot = 0;
+  CK(cudaMemGetInfo(&fre, &tot));
+  g.arena_limit = c.arena_bytes ? c.arena_bytes : (size_t)(fre * 0.9);
+  g.max_err = c.max_round_err > 0 ? c.max_round_err : 0.25;
+  g.verbose = c.verbose || getenv("BC_VERBOSE") != nullptr;
+  load_width_file(c.tune_path);
+  g.init = true;
+  return BC_OK;
+}
+
+int bc_gpu_shutdown(void) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g.init) return BC_OK;
+  cudaStreamSynchronize(g.stream);
+  for (auto &t : g.tables) cudaFree(t.second.dev);
+  g.tables.clear();
+  if (g.arena) cudaFree(g.arena);
+  g.arena = nullptr;
+  g.arena_cap = 0;
+  if (g.ev0) cudaEventDestroy(g.ev0);
+  if (g.ev1) cudaEventDestroy(g.ev1);
+  if (g.own_stream) cudaStreamDestroy(g.own_stream);
+  g_occ.clear();
+  g = Ctx();
+  return BC_OK;
+}
+
+int bc_gpu_mul(uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B, size_t BL,
+               bc_mul_stats *stats) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  bc_mul_desc d{C, CL, A, AL, B, BL};
+  bc_batch_stats st{};
+  Plan pl;
+  int r = mul_batch_locked(&d, 1, &st, &pl);
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    stats->fft_points = pl.shape.M;
+    stats->width = pl.b;
+    stats->retries = st.retries;
+    stats->max_round_err = st.max_round_err;
+    stats->device_ms = st.device_ms;
+    stats->total_ms = st.total_ms;
+  }
+  return r;
+}
+
+int bc_gpu_mul_batch(const bc_mul_desc *items, size_t n, bc_batch_stats *stats) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  bc_batch_stats st{};
+  int r = mul_batch_locked(items, n, &st);
+  if (stats) *stats = st;
+  return r;
+}
+
+int bc_gpu_set_stream(void *stream) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  g.stream = stream ? (cudaStream_t)stream : g.own_stream;
+  return BC_OK;
+}
+
+int bc_gpu_plan(size_t AL, size_t BL, size_t CL, int square, bc_plan_info *out) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!out) return BC_ERR_INVALID;
+  memset(out, 0, sizeof *out);
+  if (!CL || !AL || !BL) return BC_OK;
+  Plan pl;
+  if (!make_plan(AL, BL, CL, square != 0, 24, pl)) return BC_ERR_TOO_LARGE;
+  out->fft_points = pl.shape.M;
+  out->width = pl.b;
+  out->levels = pl.shape.levels;
+  out->L1 = pl.shape.L1;
+  out->L2 = pl.shape.L2;
+  out->Lr = pl.shape.Lr;
+  out->digits_a = pl.ndA;
+  out->digits_b = pl.square ? pl.ndA : pl.ndB;
+  out->out_words = pl.nwords;
+  out->work_bytes = work_bytes(pl);
+  return BC_OK;
+}
+
+int bc_gpu_width_limit(size_t fft_points) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return width_limit(fft_points);
+}
+
+int bc_gpu_set_width_limit(size_t fft_points, int width) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (width == 0) { g.width_override.erase(fft_points); return BC_OK; }
+  if (width < 8 || width > 24) return BC_ERR_INVALID;
+  g.width_override[fft_points] = width;
+  return BC_OK;
+}
+
+int bc_gpu_force_width(int width) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (width != 0 && (width < 8 || width > 24)) return BC_ERR_INVALID;
+  g.forced_width = width;
+  return BC_OK;
+}
+
+int bc_gpu_sync(void) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  CK(cudaStreamSynchronize(g.stream));
+  return BC_OK;
+}
+
+int bc_gpu_last_error(void) { return g.last_error; }
+int bc_gpu_last_cuda_error(void) { return g.last_cuda; }
+
+const char *bc_gpu_strerror(int code) {
+  switch (code) {
+    case BC_OK: return "ok";
+    case BC_ERR_INVALID: return "invalid argument";
+    case BC_ERR_NOMEM: return "out of device memory";
+    case BC_ERR_CUDA: return "CUDA runtime error";
+    case BC_ERR_TIMEOUT: return "carry lookback timed out";
+    case BC_ERR_PRECISION: return "rounding error above the limit at every width";
+    case BC_ERR_NOT_INIT: return "library not initialised (bc_gpu_init)";
+    case BC_ERR_TOO_LARGE: return "product too large for the supported transform lengths";
+    case BC_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case BC_ERR_CARRY: return "carry out of the top word of an exact product";
+  }
+  return "unknown error";
+}
+
+int bc_gpu_time_kernels(int on) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  g.time_kernels = on != 0;
+  g.ktimes.clear();
+  return BC_OK;
+}
+
+int bc_gpu_kernel_times(const char **names, double *ms, int cap) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  int n = 0;
+  for (auto &kt : g.ktimes) {
+    if (n >= cap) break;
+    if (names) names[n] = kt.first;
+    if (ms) ms[n] = kt.second;
+    n++;
+  }
+  return (int)g.ktimes.size();
+}
+
+}  // extern "C"

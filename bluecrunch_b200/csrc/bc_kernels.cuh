@@ -1,0 +1,528 @@
+// bc_kernels.cuh — pass kernels of the exact FFT multiply (sm_100a).
+//
+// A product class has complex length M = L1 * S1 (two levels, S1 = Lr) or
+// M = L1 * L2 * Lr (three levels).  Point n of operand X holds the balanced
+// digits n and n+M weighted by e^{i pi n/(2M)}.  Passes (one launch each,
+// every launch covers all items of the class):
+//
+//   k_outer_fwd   digits -> pre-weight -> L1-point DFT down each column of the
+//                 L1 x S1 matrix -> twiddle e^{-2 pi i s(4k1-1)/(4M)} (the
+//                 column's weight factor folded in) -> buffer
+//   k_mid<false>  (3 levels) L2-point DFT down columns of each L2 x Lr block,
+//                 twiddle e^{-2 pi i s k2/(L2 Lr)}
+//   k_rows        per row of Lr points: forward DFT of A and B, pointwise
+//                 product (or square), inverse DFT — the spectrum never
+//                 leaves the chip
+//   k_mid<true>   (3 levels) inverse of k_mid
+//   k_outer_inv   conjugate twiddle -> inverse L1-point DFT -> un-weight and
+//                 1/M -> round (max |x - round(x)| recorded) -> run records:
+//                 8 consecutive coefficients -> (H, C), value H + C*2^{8b}
+//   k_carry       decoupled-lookback scan of run carries -> output words
+//
+// k_small does all of it in one CTA for M <= 4096.
+//
+// Reference correspondence: the whole pipeline computes what _fft_mul
+// computes (bigfloat/mul.c:108-174): the exact C = A*B mod 2^{32 CL}.
+#pragma once
+#include <cuda/atomic>
+
+#include "bc_device.cuh"
+
+namespace bc {
+
+enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_TOPCARRY = 2u };
+
+struct ItemDesc {
+  const uint32_t *A;
+  const uint32_t *B;
+  uint32_t *C;
+  unsigned long long AL, BL, CL;  // AL, BL already clamped to CL
+  unsigned long long ndA, ndB;    // number of balanced digits
+  double2 *bufA;
+  double2 *bufB;                  // null when squaring
+  RunRec *rec;                    // 2M/8 run records
+  uint32_t *status;               // lookback tile status, zeroed before k_carry
+  unsigned long long nwords;      // words written by k_carry (the rest are 0)
+  unsigned long long nruns;       // runs needed to cover nwords
+  unsigned long long tile0;       // first k_carry tile of this item (class-wide numbering)
+  unsigned long long *err;        // max rounding error as double bits (atomicMax)
+  unsigned int *flags;
+  int b;
+  int square;
+};
+
+struct ClassParams {
+  int M;
+  int L1, S1;      // outer pass: L1-point DFTs with stride S1 = M/L1
+  int L2, Lr;      // 3 levels: L2-point DFTs with stride Lr; 2 levels: L2 = 1, Lr = S1
+  Tw2 tw4M;        // e^{-2 pi i m/(4M)}
+  const double2 *pw_fwd;  // e^{+i pi n1/(2 L1)}
+  const double2 *pw_inv;  // e^{-i pi n1/(2 L1)} / M
+  const double2 *twL1, *twL2, *twLr;  // e^{-2 pi i m/L}
+  const ItemDesc *items;
+  int nitems;
+  unsigned int *counter;  // k_carry dynamic tile counter (zeroed before launch)
+  unsigned long long carry_tiles;  // total k_carry tiles over the class
+};
+
+// e^{-2 pi i m/(4M)} for m = s*(4k-1) with s < S, k < 4M/(4S): m < 4M when
+// k >= 1; for k = 0 it is the conjugate of m = s.
+__device__ __forceinline__ double2 outer_tw(const Tw2 &T, int s, int k) {
+  if (k == 0) { double2 w = tw2_get(T, (uint64_t)s); return make_double2(w.x, -w.y); }
+  return tw2_get(T, (uint64_t)s * (uint64_t)(4 * k - 1));
+}
+
+__device__ __forceinline__ void atomic_max_err(unsigned long long *p, double e) {
+  // non-negative doubles order like their bit patterns
+  unsigned long long bits = (unsigned long long)__double_as_longlong(e);
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long t = __shfl_xor_sync(~0u, bits, o);
+    bits = t > bits ? t : bits;
+  }
+  if ((threadIdx.x & 31) == 0 && bits) atomicMax(p, bits);
+}
+
+// ------------------------------------------------------------------ outer fwd
+template <int L, int W>
+__global__ void __launch_bounds__((L / PTS) * W, 1) k_outer_fwd(ClassParams p) {
+  extern __shared__ double2 sm[];
+  constexpr int TC = L / PTS;
+  const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const int tiles = p.S1 / W;
+  const long long total = (long long)p.nitems * 2 * tiles;
+  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
+    const int item = (int)(unit / (2 * tiles));
+    const int rem = (int)(unit % (2 * tiles));
+    const int op = rem / tiles, tile = rem % tiles;
+    const ItemDesc &it = p.items[item];
+    if (op == 1 && it.square) continue;
+    const uint32_t *X = op ? it.B : it.A;
+    const unsigned long long XL = op ? it.BL : it.AL, nd = op ? it.ndB : it.ndA;
+    double2 *buf = op ? it.bufB : it.bufA;
+    const int col = tile * W + s;
+    double2 v[PTS];
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int n1 = t + i * TC;
+      const uint64_t n = (uint64_t)n1 * p.S1 + col;
+      double2 z = make_double2(digit_at(X, XL, it.b, n, nd), digit_at(X, XL, it.b, n + p.M, nd));
+      v[i] = cmul(z, __ldg(&p.pw_fwd[n1]));
+    }
+    block_fft<L, W, false>(v, t, s, sm, p.twL1);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int k1 = t + i * TC;
+      buf[(uint64_t)k1 * p.S1 + col] = cmul(v[i], outer_tw(p.tw4M, col, k1));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ middle (3 levels)
+template <int L, int W, bool INV>
+__global__ void __launch_bounds__((L / PTS) * W, 1) k_mid(ClassParams p) {
+  extern __shared__ double2 sm[];
+  constexpr int TC = L / PTS;
+  const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const int tiles = p.Lr / W;
+  const int nops = INV ? 1 : 2;
+  const long long per_item = (long long)nops * p.L1 * tiles;
+  const long long total = (long long)p.nitems * per_item;
+  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
+    const int item = (int)(unit / per_item);
+    long long rem = unit % per_item;
+    const int op = (int)(rem / ((long long)p.L1 * tiles));
+    rem %= (long long)p.L1 * tiles;
+    const int blk = (int)(rem / tiles), tile = (int)(rem % tiles);
+    const ItemDesc &it = p.items[item];
+    if (op == 1 && it.square) continue;
+    double2 *buf = (op ? it.bufB : it.bufA) + (uint64_t)blk * p.S1;
+    const int col = tile * W + s;
+    double2 v[PTS];
+    if (!INV) {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = buf[(uint64_t)(t + i * TC) * p.Lr + col];
+      block_fft<L, W, false>(v, t, s, sm, p.twL2);
+#pragma unroll
+      for (int i = 0; i < PTS; i++) {
+        const int k2 = t + i * TC;
+        const double2 w = tw2_get(p.tw4M, (uint64_t)4 * p.L1 * ((uint64_t)col * k2));
+        buf[(uint64_t)k2 * p.Lr + col] = cmul(v[i], w);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) {
+        const int k2 = t + i * TC;
+        const double2 w = tw2_get(p.tw4M, (uint64_t)4 * p.L1 * ((uint64_t)col * k2));
+        v[i] = cmulc(buf[(uint64_t)k2 * p.Lr + col], w);
+      }
+      block_fft<L, W, true>(v, t, s, sm, p.twL2);
+#pragma unroll
+      for (int i = 0; i < PTS; i++) buf[(uint64_t)(t + i * TC) * p.Lr + col] = v[i];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ rows
+// NR rows of Lr points per CTA; forward A (and B), product, inverse, in place
+// in bufA.
+template <int L, int NR, bool SQ>
+__global__ void __launch_bounds__((L / PTS) * NR, 1) k_rows(ClassParams p) {
+  extern __shared__ double2 sm[];
+  constexpr int TC = L / PTS, ROWE = TileSmem<L, 1>::elems;
+  const int tid = threadIdx.x, rl = tid / TC, t = tid % TC;
+  double2 *smr = sm + rl * ROWE;
+  const int rows = p.M / L;
+  const int groups = rows / NR;
+  const long long total = (long long)p.nitems * groups;
+  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
+    const int item = (int)(unit / groups);
+    const int row = (int)(unit % groups) * NR + rl;
+    const ItemDesc &it = p.items[item];
+    double2 *ra = it.bufA + (uint64_t)row * L;
+    double2 va[PTS], v[PTS];
+#pragma unroll
+    for (int i = 0; i < PTS; i++) va[i] = ra[t + i * TC];
+    block_fft<L, 1, false>(va, t, 0, smr, p.twLr);
+    if (SQ) {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = cmul(va[i], va[i]);
+    } else {
+      const double2 *rb = it.bufB + (uint64_t)row * L;
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = rb[t + i * TC];
+      block_fft<L, 1, false>(v, t, 0, smr, p.twLr);
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = cmul(va[i], v[i]);
+    }
+    block_fft<L, 1, true>(v, t, 0, smr, p.twLr);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) ra[t + i * TC] = v[i];
+  }
+}
+
+// ------------------------------------------------------------------ runs
+// 8 consecutive rounded coefficients c_u (exact integers held in doubles) ->
+// H = sum (bits of the running carry) and C = final signed carry.
+__device__ __forceinline__ void u192_or_bits(U192 &h, unsigned long long bits, int off) {
+  const int wi = off >> 6, bi = off & 63;
+  h.w[wi] |= bits << bi;
+  if (bi && wi < 2) h.w[wi + 1] |= bits >> (64 - bi);
+}
+
+__device__ __forceinline__ RunRec make_run(const double *c, int b) {
+  U192 h = {{0, 0, 0}};
+  long long acc = 0;
+  const unsigned long long mask = (1ull << b) - 1;
+#pragma unroll
+  for (int u = 0; u < 8; u++) {
+    acc += (long long)c[u];
+    u192_or_bits(h, (unsigned long long)acc & mask, b * u);
+    acc >>= b;  // arithmetic: floor division
+  }
+  RunRec r;
+  r.h0 = h.w[0]; r.h1 = h.w[1]; r.h2 = h.w[2]; r.c = acc;
+  return r;
+}
+
+__device__ __forceinline__ void store_rec(RunRec *dst, const RunRec &r) {
+  ulonglong2 *d = reinterpret_cast<ulonglong2 *>(dst);
+  d[0] = make_ulonglong2(r.h0, r.h1);
+  d[1] = make_ulonglong2(r.h2, (unsigned long long)r.c);
+}
+
+__device__ __forceinline__ RunRec load_rec(const RunRec *src) {
+  const ulonglong2 *s = reinterpret_cast<const ulonglong2 *>(src);
+  ulonglong2 a = s[0], b = s[1];
+  RunRec r;
+  r.h0 = a.x; r.h1 = a.y; r.h2 = b.x; r.c = (long long)b.y;
+  return r;
+}
+
+// ------------------------------------------------------------------ outer inv
+template <int L, int W>
+__global__ void __launch_bounds__((L / PTS) * W, 1) k_outer_inv(ClassParams p) {
+  extern __shared__ double2 sm[];
+  constexpr int TC = L / PTS, G = W / 8;
+  const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const int tiles = p.S1 / W;
+  const long long total = (long long)p.nitems * tiles;
+  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
+    const int item = (int)(unit / tiles), tile = (int)(unit % tiles);
+    const ItemDesc &it = p.items[item];
+    const int col = tile * W + s;
+    double2 v[PTS];
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int k1 = t + i * TC;
+      v[i] = cmulc(it.bufA[(uint64_t)k1 * p.S1 + col], outer_tw(p.tw4M, col, k1));
+    }
+    block_fft<L, W, true>(v, t, s, sm, p.twL1);
+    double err = 0.0;
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int n1 = t + i * TC;
+      double2 z = cmul(v[i], __ldg(&p.pw_inv[n1]));
+      double re = rint(z.x), im = rint(z.y);
+      err = fmax(err, fmax(fabs(z.x - re), fabs(z.y - im)));
+      sm[sidx<L, W>(n1, s)] = make_double2(re, im);
+    }
+    atomic_max_err(it.err, err);
+    __syncthreads();
+    // one 8-column group of one row per thread: a real run and an imaginary run
+    {
+      const int row = tid / G, g = tid % G;
+      double cre[8], cim[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        double2 z = sm[sidx<L, W>(row, 8 * g + u)];
+        cre[u] = z.x; cim[u] = z.y;
+      }
+      const uint64_t n0 = (uint64_t)row * p.S1 + (uint64_t)tile * W + 8 * g;
+      store_rec(&it.rec[n0 >> 3], make_run(cre, it.b));
+      store_rec(&it.rec[(n0 + p.M) >> 3], make_run(cim, it.b));
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ scan helper
+// Exclusive scan of transfer functions over a CTA of NT threads (earliest
+// thread first).  sw needs 65 words.  Returns the exclusive prefix; *total
+// receives the composition over the whole CTA.
+template <int NT>
+__device__ __forceinline__ uint32_t block_scan_fn(uint32_t f, uint32_t *sw, uint32_t *total) {
+  static_assert(NT % 32 == 0 && NT <= 1024, "scan CTA size");
+  constexpr int NW = NT / 32;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = f;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t o = __shfl_up_sync(~0u, inc, d);
+    if (lane >= d) inc = fn_compose(o, inc);
+  }
+  uint32_t ex = __shfl_up_sync(~0u, inc, 1);
+  if (lane == 0) ex = FN_ID;
+  if (lane == 31) sw[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t x = lane < NW ? sw[lane] : FN_ID;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t o = __shfl_up_sync(~0u, x, d);
+      if (lane >= d) x = fn_compose(o, x);
+    }
+    uint32_t wx = __shfl_up_sync(~0u, x, 1);
+    if (lane == 0) wx = FN_ID;
+    if (lane < NW) sw[32 + lane] = wx;
+    if (lane == 31) sw[64] = x;
+  }
+  __syncthreads();
+  const uint32_t r = fn_compose(sw[32 + wid], ex);
+  *total = sw[64];
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------------------ carry
+// Decoupled lookback over tiles of CARRY_NT runs.  Tile status word:
+// 0 = not ready, (1<<30)|fn = aggregate, (2<<30)|(delta+1) = inclusive.
+constexpr int CARRY_NT = 256;
+constexpr unsigned ST_AGG = 1u << 30, ST_INC = 2u << 30;
+constexpr int LOOKBACK_SPINS = 1 << 22;
+
+__device__ __forceinline__ U192 rec_h(const RunRec &r) { U192 h = {{r.h0, r.h1, r.h2}}; return h; }
+
+__device__ __forceinline__ void write_run_words(uint32_t *C, unsigned long long nwords, unsigned long long r,
+                                                int nbits, const U192 &h, const U192 &hn) {
+  const unsigned long long bit0 = r * (unsigned long long)nbits;
+  unsigned long long w = (bit0 + 31) >> 5;
+  const unsigned long long wend = (bit0 + nbits + 31) >> 5;
+  for (; w < wend && w < nwords; w++) {
+    const int off = (int)((w << 5) - bit0);
+    uint32_t x = u192_bits32(h, off);
+    if (off + 32 > nbits) x |= u192_bits32(hn, 0) << (nbits - off);
+    C[w] = x;
+  }
+}
+
+__global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
+  __shared__ uint32_t sw[65];
+  __shared__ unsigned long long s_unit;
+  __shared__ int s_delta;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_unit = atomicAdd(p.counter, 1u);
+    __syncthreads();
+    const unsigned long long unit = s_unit;
+    __syncthreads();
+    if (unit >= p.carry_tiles) break;
+    // find the item owning this tile (items are ordered by tile0)
+    int lo = 0, hi = p.nitems - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (p.items[mid].tile0 <= unit) lo = mid; else hi = mid - 1;
+    }
+    const ItemDesc &it = p.items[lo];
+    const unsigned long long tile = unit - it.tile0;
+    const unsigned long long r = tile * CARRY_NT + tid;
+    const int nbits = 8 * it.b;
+    const unsigned long long nrec = (unsigned long long)(2 * p.M) / 8;
+    U192 h = {{0, 0, 0}};
+    long long cself = 0;
+    uint32_t f = FN_ID;
+    if (r < it.nruns) {
+      RunRec rr = load_rec(&it.rec[r]);
+      h = rec_h(rr);
+      cself = rr.c;
+      const long long cprev = r ? load_rec(&it.rec[r - 1]).c : 0;
+      f = run_transfer(h, cprev, nbits);
+    }
+    uint32_t agg;
+    const uint32_t ex = block_scan_fn<CARRY_NT>(f, sw, &agg);
+    if (tid == 0) {
+      cuda::atomic_ref<uint32_t, cuda::thread_scope_device> me(it.status[tile]);
+      int din = 0;
+      if (tile == 0) {
+        me.store(ST_INC | (uint32_t)(fn_apply(agg, 0) + 1), cuda::memory_order_release);
+      } else {
+        me.store(ST_AGG | agg, cuda::memory_order_release);
+        uint32_t acc = FN_ID;  // composition of the tiles seen so far (nearest last applied)
+        long long prev = (long long)tile - 1;
+        int spins = 0;
+        bool timed_out = false;
+        for (;;) {
+          cuda::atomic_ref<uint32_t, cuda::thread_scope_device> st(it.status[prev]);
+          const uint32_t v = st.load(cuda::memory_order_acquire);
+          if (v & ST_INC) {
+            din = fn_apply(acc, (int)(v & 3u) - 1);
+            break;
+          } else if (v & ST_AGG) {
+            acc = fn_compose(v & 0x3fu, acc);
+            prev--;
+            if (prev < 0) { din = fn_apply(acc, 0); break; }
+          } else {
+            if (++spins > LOOKBACK_SPINS) { timed_out = true; break; }
+            if (spins > 32) __nanosleep(64);
+          }
+        }
+        if (timed_out) {
+          atomicOr(it.flags, FLAG_TIMEOUT);
+          din = 0;
+        }
+        me.store(ST_INC | (uint32_t)(fn_apply(agg, din) + 1), cuda::memory_order_release);
+      }
+      s_delta = din;
+    }
+    __syncthreads();
+    if (r < it.nruns) {
+      const int dprev = fn_apply(ex, s_delta);
+      const int dself = fn_apply(f, dprev);
+      u192_add_delta(h, dprev, nbits);
+      U192 hn = {{0, 0, 0}};
+      if (r + 1 < nrec) {
+        RunRec rn = load_rec(&it.rec[r + 1]);
+        hn = rec_h(rn);
+        (void)u192_add_s64(hn, cself, nbits);
+        u192_add_delta(hn, dself, nbits);
+      }
+      write_run_words(it.C, it.nwords, r, nbits, h, hn);
+      if (r + 1 == nrec && cself + dself != 0) atomicOr(it.flags, FLAG_TOPCARRY);
+    }
+    // zero any words beyond the product (CL > product length)
+    if (tile == 0) {
+      for (unsigned long long w = it.nwords + tid; w < it.CL; w += CARRY_NT) it.C[w] = 0;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ small
+// Whole product in one CTA of M/8 threads (M <= 4096): pack, FFT, product,
+// inverse, round, runs, in-CTA carry scan, words.
+template <int M, bool SQ>
+__global__ void __launch_bounds__(M / PTS, 1) k_small(ClassParams p) {
+  extern __shared__ double2 sm[];
+  constexpr int TC = M / PTS, NR = M / 8;  // NR real runs, NR imaginary runs
+  static_assert(TC % 32 == 0, "k_small needs M >= 256");
+  __shared__ uint32_t sw[65];
+  const int t = threadIdx.x;
+  RunRec *srec = reinterpret_cast<RunRec *>(sm);  // reused after the FFTs
+  for (int item = blockIdx.x; item < p.nitems; item += gridDim.x) {
+    const ItemDesc &it = p.items[item];
+    double2 va[PTS], v[PTS];
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int n = t + i * TC;
+      double2 z = make_double2(digit_at(it.A, it.AL, it.b, n, it.ndA), digit_at(it.A, it.AL, it.b, n + M, it.ndA));
+      va[i] = cmul(z, __ldg(&p.pw_fwd[n]));
+    }
+    block_fft<M, 1, false>(va, t, 0, sm, p.twL1);
+    if (SQ) {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = cmul(va[i], va[i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) {
+        const int n = t + i * TC;
+        double2 z = make_double2(digit_at(it.B, it.BL, it.b, n, it.ndB), digit_at(it.B, it.BL, it.b, n + M, it.ndB));
+        v[i] = cmul(z, __ldg(&p.pw_fwd[n]));
+      }
+      block_fft<M, 1, false>(v, t, 0, sm, p.twL1);
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = cmul(va[i], v[i]);
+    }
+    block_fft<M, 1, true>(v, t, 0, sm, p.twL1);
+    double err = 0.0;
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int n = t + i * TC;
+      double2 z = cmul(v[i], __ldg(&p.pw_inv[n]));
+      double re = rint(z.x), im = rint(z.y);
+      err = fmax(err, fmax(fabs(z.x - re), fabs(z.y - im)));
+      sm[sidx<M, 1>(n, 0)] = make_double2(re, im);
+    }
+    atomic_max_err(it.err, err);
+    __syncthreads();
+    double cre[8], cim[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      double2 z = sm[sidx<M, 1>(8 * t + u, 0)];
+      cre[u] = z.x; cim[u] = z.y;
+    }
+    RunRec rre = make_run(cre, it.b), rim = make_run(cim, it.b);
+    __syncthreads();
+    srec[t] = rre;
+    srec[NR + t] = rim;
+    __syncthreads();
+    const int nbits = 8 * it.b;
+    // transfer functions
+    U192 hre = rec_h(rre), him = rec_h(rim);
+    const long long cprev_re = t ? srec[t - 1].c : 0;
+    const long long cprev_im = srec[NR + t - 1].c;
+    const uint32_t fre = run_transfer(hre, cprev_re, nbits);
+    const uint32_t fim = run_transfer(him, cprev_im, nbits);
+    uint32_t tot_re, tot_im;
+    const uint32_t ex_re = block_scan_fn<TC>(fre, sw, &tot_re);
+    const uint32_t ex_im = block_scan_fn<TC>(fim, sw, &tot_im);
+    const int din_re = fn_apply(ex_re, 0);
+    const int d_half = fn_apply(tot_re, 0);
+    const int din_im = fn_apply(ex_im, d_half);
+    u192_add_delta(hre, din_re, nbits);
+    u192_add_delta(him, din_im, nbits);
+    const int dout_im = fn_apply(fim, din_im);
+    __syncthreads();
+    srec[t].h0 = hre.w[0]; srec[t].h1 = hre.w[1]; srec[t].h2 = hre.w[2];
+    srec[NR + t].h0 = him.w[0]; srec[NR + t].h1 = him.w[1]; srec[NR + t].h2 = him.w[2];
+    __syncthreads();
+    const U192 zero = {{0, 0, 0}};
+    const U192 nre = rec_h(srec[t + 1 < 2 * NR ? t + 1 : t]);
+    const U192 nim = (NR + t + 1 < 2 * NR) ? rec_h(srec[NR + t + 1]) : zero;
+    write_run_words(it.C, it.nwords, (unsigned long long)t, nbits, hre, nre);
+    write_run_words(it.C, it.nwords, (unsigned long long)(NR + t), nbits, him, nim);
+    if (t == TC - 1 && rim.c + dout_im != 0) atomicOr(it.flags, FLAG_TOPCARRY);
+    for (unsigned long long w = it.nwords + t; w < it.CL; w += TC) it.C[w] = 0;
+    __syncthreads();
+  }
+}
+
+}  // namespace bc

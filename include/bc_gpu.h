@@ -1,0 +1,128 @@
+/* bc_gpu.h — C ABI of libbcgpu, the B200 (sm_100a) exact multiply engine.
+ *
+ * The library computes exact products of little-endian base-2^32 integers
+ * (the limb format of bigfloat_t, include/bigfloat.h:6-13 in the reference)
+ * with an FP64 FFT convolution on one GPU.  It is what the reference's
+ * _fft_mul (include/mul.h:3, bigfloat/mul.c:108-174) becomes when it crosses
+ * to the device: include/mul.h in this repository keeps that prototype and
+ * forwards to bc_gpu_mul; batched tree levels use bc_gpu_mul_batch.
+ *
+ * All functions return BC_OK (0) or a negative BC_ERR_* code; nothing aborts.
+ * Pointers may be host memory or device memory of the selected GPU; the
+ * library detects which.  Calls are serialised internally (re-entrant).
+ */
+#ifndef BC_GPU_H
+#define BC_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  BC_OK = 0,
+  BC_ERR_INVALID = -1,     /* bad argument (null pointer with nonzero length, ...) */
+  BC_ERR_NOMEM = -2,       /* device memory could not be reserved */
+  BC_ERR_CUDA = -3,        /* a CUDA runtime call failed (see bc_gpu_last_cuda_error) */
+  BC_ERR_TIMEOUT = -4,     /* carry lookback gave up waiting (bounded spin ran out) */
+  BC_ERR_PRECISION = -5,   /* rounding error stayed >= the limit down to the minimum width */
+  BC_ERR_NOT_INIT = -6,    /* bc_gpu_init has not succeeded */
+  BC_ERR_TOO_LARGE = -7,   /* product needs a transform longer than supported (2^30 points) */
+  BC_ERR_NO_DEVICE = -8,   /* no usable sm_100 device */
+  BC_ERR_CARRY = -9        /* carry out of the top word of an exact product (internal check) */
+};
+
+/* Configuration for bc_gpu_init; a NULL pointer means all defaults. */
+typedef struct {
+  int device;             /* CUDA device ordinal (default 0) */
+  size_t arena_bytes;     /* device work arena cap; 0 = 90% of free memory at init */
+  const char *tune_path;  /* width table file (bc_tune format); NULL = built-in/env BC_TUNE_FILE */
+  double max_round_err;   /* retry threshold on max |x - round(x)| (default 0.25) */
+  int verbose;            /* 1: print plans and retries to stderr */
+} bc_gpu_config;
+
+/* Per-product statistics (optional out-parameter). */
+typedef struct {
+  int width;              /* bits per balanced digit actually used */
+  int retries;            /* times the product was redone at a narrower width */
+  size_t fft_points;      /* complex transform length M (2M real coefficients) */
+  double max_round_err;   /* max |x - round(x)| over all 2M coefficients */
+  double device_ms;       /* GPU time of the kernels (CUDA events) */
+  double total_ms;        /* wall time of the call including copies */
+} bc_mul_stats;
+
+/* One independent product of a batch.  C receives exactly CL words of
+ * A*B mod 2^(32*CL).  C may alias its own A or B (all inputs are read before
+ * any output is written); items must not alias each other's outputs. */
+typedef struct {
+  uint32_t *C;
+  size_t CL;
+  const uint32_t *A;
+  size_t AL;
+  const uint32_t *B;
+  size_t BL;
+} bc_mul_desc;
+
+typedef struct {
+  size_t items;
+  size_t classes;         /* distinct transform shapes launched */
+  size_t launches;        /* kernel launches issued (per attempt) */
+  int retries;            /* items redone at a narrower width */
+  double max_round_err;
+  double device_ms;       /* GPU time of the kernels */
+  double total_ms;        /* wall time including copies */
+  size_t h2d_bytes, d2h_bytes;
+} bc_batch_stats;
+
+/* Plan of one product (no GPU needed; for inspection and tests). */
+typedef struct {
+  size_t fft_points;      /* M */
+  int width;              /* b */
+  int levels;             /* 1 = single-CTA kernel, 2 or 3 = passes over HBM */
+  int L1, L2, Lr;         /* decomposition M = L1 * L2 * Lr (L2 = 1 for two levels) */
+  size_t digits_a, digits_b;
+  size_t out_words;       /* words produced by the transform (the rest are 0) */
+  size_t work_bytes;      /* device scratch for this product */
+} bc_plan_info;
+
+int bc_gpu_init(const bc_gpu_config *cfg);
+int bc_gpu_shutdown(void);
+
+/* C[0..CL) = A*B mod 2^(32*CL).  AL, BL >= 0 (a zero length means zero).
+ * Same semantics as _fft_mul (bigfloat/mul.c:108-174) minus its aborts. */
+int bc_gpu_mul(uint32_t *C, size_t CL, const uint32_t *A, size_t AL,
+               const uint32_t *B, size_t BL, bc_mul_stats *stats);
+
+/* Independent products in as few launches as their shapes allow: items are
+ * bucketed by transform length and every pass covers a whole bucket. */
+int bc_gpu_mul_batch(const bc_mul_desc *items, size_t n, bc_batch_stats *stats);
+
+/* Launch on this CUDA stream (cudaStream_t as void*; NULL = library stream).
+ * Calls still return only when their results are complete. */
+int bc_gpu_set_stream(void *stream);
+
+int bc_gpu_plan(size_t AL, size_t BL, size_t CL, int square, bc_plan_info *out);
+
+/* Largest width allowed at transform length M by the loaded width table. */
+int bc_gpu_width_limit(size_t fft_points);
+/* Override the width limit for one transform length (autotuner); 0 = reset. */
+int bc_gpu_set_width_limit(size_t fft_points, int width);
+
+/* Force the width of subsequent products (0 = automatic); for error sweeps. */
+int bc_gpu_force_width(int width);
+
+int bc_gpu_sync(void);
+int bc_gpu_last_error(void);
+int bc_gpu_last_cuda_error(void);
+const char *bc_gpu_strerror(int code);
+
+/* Per-kernel GPU time of the last bc_gpu_mul / bc_gpu_mul_batch when kernel
+ * timing is on (bc_gpu_time_kernels(1)).  names[i] / ms[i], returns count. */
+int bc_gpu_time_kernels(int on);
+int bc_gpu_kernel_times(const char **names, double *ms, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

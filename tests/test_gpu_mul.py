@@ -1,0 +1,113 @@
+"""GPU parity: bc_gpu_mul / bc_gpu_mul_batch (the device side of _fft_mul,
+bigfloat/mul.c:108-174) against the oracle.  Bit-exact throughout."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import exact, limbs
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _check(gpu, orc, a, b, CL=None, square=False):
+    CL = CL or (len(a) + len(b))
+    c, st = gpu.mul(a, None if square else b, CL=CL, square=square, want_stats=True)
+    if CL <= 20000:
+        want = exact(a, a if square else b, CL)
+    else:
+        want = orc.ntt_mul(a, a if square else b, CL)
+    assert np.array_equal(c, want), (len(a), len(b), CL, st)
+    assert st["max_round_err"] < 0.25
+    return st
+
+
+@pytest.mark.parametrize("al,bl", [(1, 1), (1, 7), (3, 5), (13, 100), (50, 50), (100, 100), (255, 257),
+                                   (1000, 1000), (1000, 125), (4096, 4096), (6000, 3000)])
+def test_small_and_medium(gpu, orc, al, bl):
+    _check(gpu, orc, limbs(al * 7 + 1, al), limbs(bl * 7 + 2, bl))
+
+
+@pytest.mark.parametrize("al,bl", [(10000, 10000), (16384, 16384), (40000, 5000), (65536, 65536),
+                                   (100000, 100000), (131072, 16384), (262144, 262144)])
+def test_two_level(gpu, orc, al, bl):
+    _check(gpu, orc, limbs(al + 11, al), limbs(bl + 13, bl))
+
+
+@pytest.mark.parametrize("al", [1 << 19, 1 << 20, 3 << 19])
+def test_three_level(gpu, orc, al):
+    _check(gpu, orc, limbs(al + 17, al), limbs(al + 19, al))
+
+
+@pytest.mark.parametrize("n", [100, 2048, 30000, 1 << 18, 1 << 20])
+def test_squaring(gpu, orc, n):
+    a = limbs(n + 23, n)
+    _check(gpu, orc, a, a, square=True)
+
+
+def test_golden_products(gpu):
+    import hashlib
+    import oracle
+    g = json.load(open(os.path.join(HERE, "golden", "products.json")))
+    for case in g["cases"]:
+        a = oracle.random_limbs(case["seed_a"], case["AL"])
+        b = a if case["square"] else oracle.random_limbs(case["seed_b"], case["BL"])
+        c = gpu.mul(a, None if case["square"] else b, CL=case["CL"], square=case["square"])
+        assert hashlib.sha256(c.astype("<u4").tobytes()).hexdigest() == case["sha256"], case
+
+
+def test_edge_values(gpu, orc):
+    for n in (100, 5000, 70000):
+        ones = np.full(n, 0xFFFFFFFF, dtype=np.uint32)
+        _check(gpu, orc, ones, ones)
+        _check(gpu, orc, ones, ones, square=True)
+        alt = np.tile(np.array([0x80008000, 0x7FFF7FFF], dtype=np.uint32), n // 2)
+        _check(gpu, orc, alt, alt)
+        z = np.zeros(n, dtype=np.uint32); z[-1] = 1
+        _check(gpu, orc, z, ones)
+
+
+def test_truncated_and_padded_outputs(gpu, orc):
+    a, b = limbs(5, 3000), limbs(6, 2000)
+    _check(gpu, orc, a, b, CL=6000)      # CL > AL+BL: high words zero
+    _check(gpu, orc, a, b, CL=2500)      # CL < AL+BL: low words only
+    _check(gpu, orc, a, b, CL=1)
+
+
+def test_zero_length(gpu):
+    c = gpu.mul(np.zeros(0, dtype=np.uint32), limbs(1, 10), CL=12)
+    assert not c.any()
+
+
+def test_batch_matches_single(gpu, orc):
+    rng = np.random.default_rng(7)
+    items = []
+    for i in range(40):
+        al = int(np.exp(rng.uniform(np.log(64), np.log(60000))))
+        bl = int(np.exp(rng.uniform(np.log(64), np.log(60000))))
+        a = limbs(1000 + i, al)
+        b = a if i % 5 == 0 else limbs(2000 + i, bl)
+        items.append((a, None if i % 5 == 0 else b, None))
+    outs, st = gpu.mul_batch(items, want_stats=True)
+    for (a, b, _), c in zip(items, outs):
+        bb = a if b is None else b
+        assert np.array_equal(c, orc.ntt_mul(a, bb, len(a) + len(bb)))
+    assert st["classes"] >= 2
+
+
+def test_device_pointers_and_aliasing(gpu, orc):
+    torch = pytest.importorskip("torch")
+    a, b = limbs(31, 50000), limbs(32, 40000)
+    da = torch.from_numpy(a.view(np.int32)).cuda()
+    db = torch.from_numpy(b.view(np.int32)).cuda()
+    dc = torch.zeros(90000, dtype=torch.int32, device="cuda")
+    gpu.mul(da, db, CL=90000, out=dc)
+    want = orc.ntt_mul(a, b)
+    assert np.array_equal(dc.cpu().numpy().view(np.uint32), want)
+    # in place: C aliases A (bigfloat_mul's in-place path, bigfloat/mul.c:609-627)
+    buf = torch.zeros(90000, dtype=torch.int32, device="cuda")
+    buf[:50000] = da
+    gpu.mul(buf[:50000], db, CL=90000, out=buf)
+    assert np.array_equal(buf.cpu().numpy().view(np.uint32), want)
