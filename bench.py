@@ -1,0 +1,379 @@
+#!/usr/bin/env python3
+"""Benchmark: exact bigfloat multiply throughput on B200 (and the reference
+CPU multiply beside it).
+
+Workload (the "single exact bigfloat multiply" configuration): A, B of
+2^24 uniformly random base-2^32 limbs each (SplitMix64, seed 0xB1C0FFEE ^
+log2(len), top limb nonzero), C = A*B of 2^25 limbs, bit-exact.  One step is
+one product.  Operands and FFT work buffers (GBs) are far larger than the
+126 MB L2, so no flush is needed between steps.
+
+Metric: exact-multiply GB/s by the fixed algorithmic-bytes formula
+    bytes = 4(AL+BL+CL) + (3-s) * 2 * 32 * Nc,  Nc = ceil(32 CL / b)/2
+with b the width limit of the chosen transform length (the widest digits
+that pass the 0.25 rounding-error criterion) and s = 1 for squaring.
+`value` times device-resident operands; `e2e` times the C ABI call with
+pinned host buffers (copies inside the timed region).
+
+Reference arm (--impl reference): the reference's own _fft_mul compiled from
+its sources (oracle/_ref, OpenMP tasks over all host threads), on the largest
+size its packers support (2^20 x 2^20 limbs; it aborts for CL > 4e6), same
+formula and unit.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+SEED = 0xB1C0FFEE
+HEADLINE_LOG2 = 24
+REF_LOG2 = 20
+
+
+def alg_bytes(AL, BL, CL, b, square):
+    nc = math.ceil(32 * CL / b) / 2
+    return 4 * (AL + BL + CL) + (3 - (1 if square else 0)) * 2 * 32 * nc
+
+
+def operands(log2n, square=False, ratio=1):
+    import oracle
+    n = 1 << log2n
+    a = oracle.random_limbs(SEED ^ log2n, n)
+    b = a if square else oracle.random_limbs((SEED ^ log2n) + 1, n // ratio)
+    return a, b
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- reference arm
+def time_reference(log2n=REF_LOG2, reps=3, kind="omp"):
+    import oracle
+    ref = oracle.reference(kind)
+    a, b = operands(log2n)
+    CL = a.size + b.size
+    ref.fft_mul(a, b, CL, parallel=(kind == "omp"))  # warm (tables)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ref.fft_mul(a, b, CL, parallel=(kind == "omp"))
+    dt = (time.perf_counter() - t0) / reps
+    return a.size, b.size, CL, dt, ref.threads()
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.have_reference("omp"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}))
+        return
+    import bluecrunch_b200 as bc
+    K, W = args.steps, args.warmup
+    ref = oracle.reference("omp")
+    a, b = operands(REF_LOG2)
+    CL = a.size + b.size
+    for _ in range(W):
+        ref.fft_mul(a, b, CL, parallel=True)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        ref.fft_mul(a, b, CL, parallel=True)
+    dt = (time.perf_counter() - t0) / K
+    p = bc.plan(a.size, b.size, CL)
+    b_alg = bc.width_limit(p["fft_points"])
+    gbs = alg_bytes(a.size, b.size, CL, b_alg, False) / dt / 1e9
+    threads = ref.threads()
+    print(json.dumps({
+        "impl": "reference", "metric": "exact_mul_GBps", "value": round(gbs, 4), "unit": "GB/s",
+        "higher_is_better": True, "n_gpus": args.gpus, "steps": K, "warmup": W,
+        "ms_per_step": round(dt * 1e3, 3), "dtype": "f64", "data": "synthetic",
+        "scaling": "weak",
+        "config": {"workload": "exact multiply 2^20 x 2^20 limbs (largest size the reference packers support)",
+                   "AL": a.size, "BL": b.size, "CL": CL, "width_for_formula": b_alg},
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "reference",
+                         "sample": "reference _fft_mul (bigfloat/mul.c:108-174) from oracle/_ref, OpenMP tasks, "
+                                   "%d threads, %d timed multiplies of 2^20 x 2^20 limbs" % (threads, K)},
+        "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def gpu_arm(args):
+    import torch
+    import bluecrunch_b200 as bc
+    import oracle
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    bc.init(local)
+    stream = torch.cuda.current_stream()
+    bc.set_stream(stream.cuda_stream)
+
+    K, W = args.steps, args.warmup
+    log2n = args.log2
+    a, b = operands(log2n)
+    AL, BL = a.size, b.size
+    CL = AL + BL
+    p = bc.plan(AL, BL, CL)
+    b_alg = bc.width_limit(p["fft_points"])
+    nbytes = alg_bytes(AL, BL, CL, b_alg, False)
+
+    da = torch.from_numpy(a.view(np.int32)).cuda()
+    db = torch.from_numpy(b.view(np.int32)).cuda()
+    dc = torch.zeros(CL, dtype=torch.int32, device="cuda")
+    want_sum = None
+    # correctness of this exact workload: modular check (FP64-free) on the result
+    c, st = bc.mul(da, db, CL=CL, out=dc, want_stats=True)
+    host_c = dc.cpu().numpy().view(np.uint32)
+    assert oracle.restated().modcheck(host_c, a, b, 4), "GPU product fails the modular check"
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(W):
+        bc.mul(da, db, CL=CL, out=dc)
+    bc.time_kernels(True)
+    barrier()
+    kern = {}
+    launches = 0
+    with Clocks(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            _, st = bc.mul(da, db, CL=CL, out=dc, want_stats=True)
+            for name, ms in bc.kernel_times():
+                kern.setdefault(name, []).append(ms)
+                launches += 1
+        e1.record(stream)
+        barrier()
+    bc.time_kernels(False)
+    ms = e0.elapsed_time(e1) / K
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = nbytes * world / (ms * 1e-3) / 1e9
+
+    # ---- e2e: pinned host buffers through the C ABI, copies in the timed region
+    ha = torch.from_numpy(a.view(np.int32)).pin_memory()
+    hb = torch.from_numpy(b.view(np.int32)).pin_memory()
+    hc = torch.zeros(CL, dtype=torch.int32).pin_memory()
+    bc.mul(ha, hb, CL=CL, out=hc)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(1, K)):
+        bc.mul(ha, hb, CL=CL, out=hc)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / max(1, K)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert np.array_equal(hc.numpy().view(np.uint32), host_c)
+    e2e = nbytes * world / (e2e_ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel (algorithmic bytes per launch)
+    M = p["fft_points"]
+    per_kernel_bytes = {
+        "outer_fwd": 4 * (AL + BL) + 2 * 16 * M,
+        "mid_fwd": 2 * 2 * 16 * M,
+        "rows": 3 * 16 * M,
+        "mid_inv": 2 * 16 * M,
+        "outer_inv": 16 * M + 8 * M,
+        "carry": 8 * M + 4 * CL,
+        "small": 4 * (AL + BL + CL),
+    }
+    avg = {k: float(np.mean(v)) for k, v in kern.items()}
+    dom = max(avg, key=avg.get) if avg else None
+    peak, peak_kind = peaks()
+    roof = None
+    if dom:
+        achieved = per_kernel_bytes.get(dom, 0) / (avg[dom] * 1e-3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tf):
+            tr = json.load(open(tf)).get(dom)
+            if tr and tr.get("fft_points") == M:
+                traffic = tr.get("dram_bytes_per_launch")
+        roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": per_kernel_bytes.get(dom),
+                "kernel_ms": {k: round(v, 4) for k, v in avg.items()},
+                "kernel_share": {k: round(v / sum(avg.values()), 4) for k, v in avg.items()}}
+
+    # ---- sweep (device-resident, a few steps each)
+    sweep = []
+    if not args.no_sweep and rank == 0:
+        for lg, ratio, sq in [(14, 1, False), (16, 1, False), (18, 1, False), (20, 1, False), (22, 1, False),
+                              (24, 1, False), (26, 1, False), (27, 1, False),
+                              (20, 8, False), (24, 8, False), (27, 8, False),
+                              (20, 1, True), (24, 1, True), (27, 1, True)]:
+            try:
+                sa, sb = operands(lg, square=sq, ratio=ratio)
+                sCL = sa.size + sb.size
+                xa = torch.from_numpy(sa.view(np.int32)).cuda()
+                xb = xa if sq else torch.from_numpy(sb.view(np.int32)).cuda()
+                xc = torch.zeros(sCL, dtype=torch.int32, device="cuda")
+                _, s0 = bc.mul(xa, None if sq else xb, CL=sCL, square=sq, out=xc, want_stats=True)
+                reps = 5 if lg <= 24 else 2
+                torch.cuda.synchronize()
+                f0 = torch.cuda.Event(enable_timing=True)
+                f1 = torch.cuda.Event(enable_timing=True)
+                f0.record(stream)
+                for _ in range(reps):
+                    bc.mul(xa, None if sq else xb, CL=sCL, square=sq, out=xc)
+                f1.record(stream)
+                torch.cuda.synchronize()
+                sms = f0.elapsed_time(f1) / reps
+                sp = bc.plan(sa.size, sb.size, sCL, square=sq)
+                sb_alg = bc.width_limit(sp["fft_points"])
+                g = alg_bytes(sa.size, sb.size, sCL, sb_alg, sq) / (sms * 1e-3) / 1e9
+                ok = oracle.restated().modcheck(xc.cpu().numpy().view(np.uint32), sa, sa if sq else sb, 2)
+                sweep.append({"AL": sa.size, "BL": sb.size, "square": sq, "M": sp["fft_points"],
+                              "levels": sp["levels"], "width": s0["width"], "max_round_err": s0["max_round_err"],
+                              "ms": round(sms, 4), "GBps": round(g, 1), "frac_hbm": round(g / peak, 4),
+                              "modcheck": ok})
+                del xa, xb, xc
+                torch.cuda.empty_cache()
+            except Exception as exc:  # report, keep going
+                sweep.append({"log2": lg, "ratio": ratio, "square": sq, "error": str(exc)[:200]})
+
+    # ---- CPU baseline: the reference multiply on the host cores, bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle as orc
+        if orc.have_reference("omp"):
+            ral, rbl, rcl, rdt, thr = time_reference(REF_LOG2, reps=3, kind="omp")
+            rp = bc.plan(ral, rbl, rcl)
+            rb_alg = bc.width_limit(rp["fft_points"])
+            cpu = {"value": round(alg_bytes(ral, rbl, rcl, rb_alg, False) / rdt / 1e9, 4), "unit": "GB/s",
+                   "cores": thr, "kind": "reference",
+                   "sample": "reference _fft_mul from oracle/_ref (OpenMP tasks, %d threads), 3 multiplies of "
+                             "2^20 x 2^20 limbs (largest size it supports), %.3f s each" % (thr, rdt)}
+        else:
+            sa, sb = operands(16)
+            t0 = time.perf_counter()
+            orc.restated().fft_mul(sa, sb)
+            dt = time.perf_counter() - t0
+            rp = bc.plan(sa.size, sb.size, sa.size + sb.size)
+            cpu = {"value": round(alg_bytes(sa.size, sb.size, sa.size + sb.size, bc.width_limit(rp["fft_points"]), False) / dt / 1e9, 4),
+                   "unit": "GB/s", "cores": 1, "kind": "port", "sample": "oracle restatement, one 2^16 x 2^16 multiply"}
+
+    if rank == 0:
+        line = {
+            "metric": "exact_mul_GBps", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "exact multiply 2^%d x 2^%d limbs (SplitMix64 seeded, uniform limbs)" % (log2n, log2n),
+                       "AL": AL, "BL": BL, "CL": CL, "fft_points": M, "levels": p["levels"],
+                       "width": st["width"], "width_for_formula": b_alg, "max_round_err": st["max_round_err"],
+                       "l2": "inputs and work buffers larger than L2 (no flush)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "e2e": {"value": round(e2e, 2), "unit": "GB/s", "ms_per_step": round(e2e_ms, 3),
+                    "h2d_bytes_per_step": 4 * (AL + BL), "d2h_bytes_per_step": 4 * CL,
+                    "path": "bc_gpu_mul with pinned host buffers"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "sweep": sweep,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bluecrunch_b200")
+    ap.add_argument("--log2", type=int, default=HEADLINE_LOG2)
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -80,6 +80,8 @@ GPU_SYMBOLS = {
     "bc_gpu_width_limit": (ctypes.c_int, [_sz]),
     "bc_gpu_set_width_limit": (ctypes.c_int, [_sz, ctypes.c_int]),
     "bc_gpu_force_width": (ctypes.c_int, [ctypes.c_int]),
+    "bc_gpu_force_plan": (ctypes.c_int, [_sz, ctypes.c_int]),
+    "bc_gpu_lengths": (ctypes.c_int, [ctypes.POINTER(_sz), ctypes.c_int]),
     "bc_gpu_sync": (ctypes.c_int, []),
     "bc_gpu_last_error": (ctypes.c_int, []),
     "bc_gpu_last_cuda_error": (ctypes.c_int, []),
@@ -199,6 +201,18 @@ def set_width_limit(M, width):
 
 def force_width(width):
     _check(_lib().bc_gpu_force_width(width))
+
+
+def force_plan(fft_points, width):
+    _check(_lib().bc_gpu_force_plan(fft_points, width))
+
+
+def lengths():
+    """Supported transform lengths M (2^k and 3*2^k with a kernel shape)."""
+    n = _lib().bc_gpu_lengths(None, 0)
+    buf = (_sz * n)()
+    _lib().bc_gpu_lengths(buf, n)
+    return list(buf)
 
 
 def set_stream(ptr):

@@ -304,6 +304,9 @@ __device__ __forceinline__ uint32_t fn_make(int vm, int v0, int vp) {
   return (uint32_t)(vm + 1) | ((uint32_t)(v0 + 1) << 2) | ((uint32_t)(vp + 1) << 4);
 }
 constexpr uint32_t FN_ID = 0u | (1u << 2) | (2u << 4);
+__device__ __forceinline__ bool fn_is_const(uint32_t f) {
+  return (f & 3u) == ((f >> 2) & 3u) && (f & 3u) == ((f >> 4) & 3u);
+}
 // result = second(first(x))
 __device__ __forceinline__ uint32_t fn_compose(uint32_t first, uint32_t second) {
   return fn_make(fn_apply(second, fn_apply(first, -1)), fn_apply(second, fn_apply(first, 0)),

@@ -105,6 +105,7 @@ struct Ctx {
   std::map<size_t, int> width_override;
   std::map<size_t, int> width_file;
   int forced_width = 0;
+  size_t forced_M = 0;
   double max_err = 0.25;
   int verbose = 0;
   int last_error = 0;
@@ -195,6 +196,7 @@ bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl)
   double best = 0;
   size_t first_fit = 0;
   for (size_t M : lengths()) {
+    if (g.forced_M && M != g.forced_M) continue;
     if (first_fit && M > 4 * first_fit) break;
     int bmax = std::min(width_limit(M), bcap);
     if (g.forced_width) bmax = g.forced_width;
@@ -722,9 +724,9 @@ int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Pla
     }
     for (Work *w : todo) {
       if (w->flags & FLAG_TIMEOUT) return fail(BC_ERR_TIMEOUT);
-      st->max_round_err = std::max(st->max_round_err, w->err);
       const bool bad = !(w->err < g.max_err) || (w->flags & FLAG_TOPCARRY);
       if (!bad || g.forced_width) {
+        st->max_round_err = std::max(st->max_round_err, w->err);  // of the accepted attempt
         if (w->flags & FLAG_TOPCARRY) return fail(BC_ERR_CARRY);
         w->done = true;
         continue;
@@ -870,6 +872,22 @@ int bc_gpu_set_width_limit(size_t fft_points, int width) {
 int bc_gpu_force_width(int width) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (width != 0 && (width < 8 || width > 24)) return BC_ERR_INVALID;
+  g.forced_width = width;
+  return BC_OK;
+}
+
+int bc_gpu_lengths(size_t *out, int cap) {
+  const std::vector<size_t> &v = lengths();
+  for (int i = 0; i < cap && i < (int)v.size(); i++) out[i] = v[i];
+  return (int)v.size();
+}
+
+int bc_gpu_force_plan(size_t fft_points, int width) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (width != 0 && (width < 8 || width > 24)) return BC_ERR_INVALID;
+  Shape s;
+  if (fft_points && !shape_for(fft_points, s)) return BC_ERR_INVALID;
+  g.forced_M = fft_points;
   g.forced_width = width;
   return BC_OK;
 }

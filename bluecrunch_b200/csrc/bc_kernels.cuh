@@ -72,6 +72,16 @@ __device__ __forceinline__ double2 outer_tw(const Tw2 &T, int s, int k) {
   return tw2_get(T, (uint64_t)s * (uint64_t)(4 * k - 1));
 }
 
+// Rounding check of one point: max |x - round(x)| of its two coefficients,
+// or 1.0 when a coefficient reaches 2^50 — beyond that the distance to the
+// nearest integer stops measuring the error (doubles near 2^53 hold no
+// fractions), so the product must be redone with narrower digits.
+__device__ __forceinline__ double round_check(double2 z, double re, double im) {
+  const double big = 1125899906842624.0;  // 2^50
+  double e = fmax(fabs(z.x - re), fabs(z.y - im));
+  return (fabs(re) >= big || fabs(im) >= big) ? 1.0 : e;
+}
+
 __device__ __forceinline__ void atomic_max_err(unsigned long long *p, double e) {
   // non-negative doubles order like their bit patterns
   unsigned long long bits = (unsigned long long)__double_as_longlong(e);
@@ -263,7 +273,7 @@ __global__ void __launch_bounds__((L / PTS) * W, 1) k_outer_inv(ClassParams p) {
       const int n1 = t + i * TC;
       double2 z = cmul(v[i], __ldg(&p.pw_inv[n1]));
       double re = rint(z.x), im = rint(z.y);
-      err = fmax(err, fmax(fabs(z.x - re), fabs(z.y - im)));
+      err = fmax(err, round_check(z, re, im));
       sm[sidx<L, W>(n1, s)] = make_double2(re, im);
     }
     atomic_max_err(it.err, err);
@@ -380,13 +390,18 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
     uint32_t agg;
     const uint32_t ex = block_scan_fn<CARRY_NT>(f, sw, &agg);
     if (tid == 0) {
+      // A tile whose composed map is constant knows its carry out before its
+      // carry in: it publishes that at once, and a lookback that meets such an
+      // aggregate can stop there.  Nearly every tile is constant, so waits are
+      // one status read deep.
       cuda::atomic_ref<uint32_t, cuda::thread_scope_device> me(it.status[tile]);
       int din = 0;
       if (tile == 0) {
         me.store(ST_INC | (uint32_t)(fn_apply(agg, 0) + 1), cuda::memory_order_release);
       } else {
-        me.store(ST_AGG | agg, cuda::memory_order_release);
-        uint32_t acc = FN_ID;  // composition of the tiles seen so far (nearest last applied)
+        if (fn_is_const(agg)) me.store(ST_INC | (uint32_t)(fn_apply(agg, 0) + 1), cuda::memory_order_release);
+        else me.store(ST_AGG | agg, cuda::memory_order_release);
+        uint32_t acc = FN_ID;  // maps of the tiles passed so far (nearest applied last)
         long long prev = (long long)tile - 1;
         int spins = 0;
         bool timed_out = false;
@@ -397,19 +412,20 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
             din = fn_apply(acc, (int)(v & 3u) - 1);
             break;
           } else if (v & ST_AGG) {
-            acc = fn_compose(v & 0x3fu, acc);
+            const uint32_t fv = v & 0x3fu;
+            if (fn_is_const(fv)) { din = fn_apply(acc, fn_apply(fv, 0)); break; }
+            acc = fn_compose(fv, acc);
             prev--;
-            if (prev < 0) { din = fn_apply(acc, 0); break; }
           } else {
             if (++spins > LOOKBACK_SPINS) { timed_out = true; break; }
-            if (spins > 32) __nanosleep(64);
+            if (spins > 64) __nanosleep(32);
           }
         }
         if (timed_out) {
           atomicOr(it.flags, FLAG_TIMEOUT);
           din = 0;
         }
-        me.store(ST_INC | (uint32_t)(fn_apply(agg, din) + 1), cuda::memory_order_release);
+        if (!fn_is_const(agg)) me.store(ST_INC | (uint32_t)(fn_apply(agg, din) + 1), cuda::memory_order_release);
       }
       s_delta = din;
     }
@@ -478,7 +494,7 @@ __global__ void __launch_bounds__(M / PTS, 1) k_small(ClassParams p) {
       const int n = t + i * TC;
       double2 z = cmul(v[i], __ldg(&p.pw_inv[n]));
       double re = rint(z.x), im = rint(z.y);
-      err = fmax(err, fmax(fabs(z.x - re), fabs(z.y - im)));
+      err = fmax(err, round_check(z, re, im));
       sm[sidx<M, 1>(n, 0)] = make_double2(re, im);
     }
     atomic_max_err(it.err, err);

@@ -1,0 +1,37 @@
+/* bc_host.h — internal declarations shared by the host C sources. */
+#ifndef BC_HOST_H
+#define BC_HOST_H
+#include <stddef.h>
+#include <stdint.h>
+
+#include "bigfloat.h"
+
+/* Below this many output limbs a product stays on the host, as the
+ * reference's bigfloat_mul dispatch does (KARATZUBA_THRESH,
+ * bigfloat/mul.c:14,645-648). */
+#define BC_SMALL_PRODUCT_LIMBS 100
+
+typedef struct {
+  const uint32_t *T;
+  size_t L;
+  int64_t exp;
+} bc_operand;
+
+typedef struct {
+  uint32_t *C;
+  size_t CL;
+  const uint32_t *A;
+  size_t AL;
+  const uint32_t *B;
+  size_t BL;
+} bc_gpu_item;
+
+void *bc_xmalloc(size_t n);
+void *bc_xrealloc(void *p, size_t n);
+void bc_mul_operands(const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p, bc_operand *oa, bc_operand *ob);
+/* All items on the GPU in one batch; aborts with a message on failure. */
+void bc_host_gpu_batch(bc_gpu_item *items, size_t n);
+/* Product of small operands on the host (schoolbook), CT may alias. */
+void bc_small_mul(uint32_t *CT, size_t CL, const uint32_t *AT, size_t AL, const uint32_t *BT, size_t BL);
+
+#endif

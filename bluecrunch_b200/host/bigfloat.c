@@ -1,0 +1,343 @@
+/* bigfloat.c — bigfloat_t management, addition, subtraction, multiply
+ * dispatch and scalar multiplies.
+ *
+ * Values and lengths follow the reference bit for bit (every product is
+ * exact, so e's digits depend only on these host-side rules):
+ *   - precision p means p+2 limbs kept, low limbs chopped
+ *     (bigfloat/addsub.c:83-86,140-143, bigfloat/mul.c:573-602);
+ *   - a product has AL+BL limbs, then one top zero limb is trimmed and, above
+ *     1000 limbs, all top zero limbs (bigfloat/mul.c:667-675);
+ *   - subtraction strips top zero limbs (bigfloat/addsub.c:165-173).
+ * Memory handling is this file's own: results are built in fresh buffers and
+ * swapped in, so aliasing of target and operands is always safe.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "bigfloat.h"
+#include "bc_host.h"
+#include "mul.h"
+
+/* ---------------------------------------------------------------- lifecycle
+ * bigfloat/new.c, free.c, alloc.c, copy.c, set.c, zero.c, neg.c, floor.c */
+
+void bigfloat_new(bigfloat_t t) {
+  t->sign = 1;
+  t->exp = 0;
+  t->len = 0;
+  t->coef = NULL;
+}
+
+void bigfloat_free(bigfloat_t t) {
+  free(t->coef);
+  t->coef = NULL;
+}
+
+void bigfloat_alloc(bigfloat_t t, size_t size) {
+  bigfloat_free(t);
+  t->exp = 0;
+  t->sign = 1;
+  t->len = size;
+  t->coef = (uint32_t *)bc_xmalloc(size * sizeof(uint32_t));
+}
+
+void bigfloat_realloc(bigfloat_t t, size_t size) {
+  size_t old = t->len;
+  t->coef = (uint32_t *)bc_xrealloc(t->coef, size * sizeof(uint32_t));
+  t->len = size;
+  if (size > old) memset(t->coef + old, 0, (size - old) * sizeof(uint32_t));
+}
+
+void bigfloat_copy(bigfloat_t t, const bigfloat_t s) {
+  uint32_t *c = (uint32_t *)bc_xmalloc(s->len * sizeof(uint32_t));
+  if (s->len) memcpy(c, s->coef, s->len * sizeof(uint32_t));
+  free(t->coef);
+  t->coef = c;
+  t->exp = s->exp;
+  t->sign = s->sign;
+  t->len = s->len;
+}
+
+void bigfloat_zero(bigfloat_t t) {
+  free(t->coef);
+  t->coef = NULL;
+  t->exp = 0;
+  t->len = 0;
+  t->sign = 1;
+}
+
+int bigfloat_iszero(const bigfloat_t t) { return t->len == 0; }
+
+void bigfloat_set(bigfloat_t t, uint32_t value) {
+  if (value == 0) {
+    bigfloat_zero(t);
+    return;
+  }
+  bigfloat_alloc(t, 1);
+  t->coef[0] = value;
+}
+
+void bigfloat_neg(bigfloat_t t) {
+  if (!bigfloat_iszero(t)) t->sign = !t->sign;
+}
+
+void bigfloat_floor(bigfloat_t t) {
+  if (!t->coef || t->exp >= 0) return;
+  size_t shift = (size_t)(-t->exp);
+  t->len -= shift;
+  t->exp = 0;
+  memmove(t->coef, t->coef + shift, t->len * sizeof(uint32_t));
+  t->coef = (uint32_t *)bc_xrealloc(t->coef, t->len * sizeof(uint32_t));
+}
+
+void bigfloat_print(const char *name, const bigfloat_t v) {
+  printf("%s = bigfloat_t {exp = %ld, len = %ld, sign = %d, coef = ", name, (long)v->exp, (long)v->len, v->sign);
+  if (!v->coef) {
+    printf("NULL");
+  } else {
+    printf("{ ");
+    for (size_t i = 0; i < v->len; i++) printf(i + 1 < v->len ? "0x%08x, " : "0x%08x", v->coef[i]);
+    printf(" }");
+  }
+  printf("}\n");
+}
+
+void bigfloat_print10(const char *name, const bigfloat_t v) {
+  printf("%s = bigfloat_t {exp = %ld, len = %ld, sign = %d, coef = ", name, (long)v->exp, (long)v->len, v->sign);
+  if (!v->coef) {
+    printf("NULL");
+  } else {
+    printf("{ ");
+    for (size_t i = 0; i < v->len; i++) printf(i + 1 < v->len ? "%d, " : "%d", v->coef[i]);
+    printf(" }");
+  }
+  printf("}\n");
+}
+
+/* ---------------------------------------------------------------- add / sub */
+
+/* Limb of x at magnitude m (0 outside), bigfloat/addsub.c:17-27. */
+static inline uint32_t limb_at(const _bigfloat_struct *x, int64_t m) {
+  if (m < x->exp || m >= x->exp + (int64_t)x->len) return 0;
+  return x->coef[m - x->exp];
+}
+
+/* Compare |a| and |b|: 1, -1 or 0 (bigfloat/addsub.c:33-63). */
+static int ucmp(const _bigfloat_struct *a, const _bigfloat_struct *b) {
+  int64_t ta = a->exp + (int64_t)a->len, tb = b->exp + (int64_t)b->len;
+  if (ta != tb) return ta > tb ? 1 : -1;
+  for (int64_t m = ta; m >= a->exp || m >= b->exp; m--) {
+    uint32_t x = limb_at(a, m), y = limb_at(b, m);
+    if (x != y) return x > y ? 1 : -1;
+  }
+  return 0;
+}
+
+/* The window [bot, top) kept for a sum or difference at precision p
+ * (bigfloat/addsub.c:65-90 and 123-145): everything when p == 0, else the top
+ * p+2 limbs.  Returns the exponent the reference assigns (top - p, with p the
+ * window length when untruncated). */
+static int64_t window(const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p, int64_t *bot, int64_t *top) {
+  int64_t ta = a->exp + (int64_t)a->len, tb = b->exp + (int64_t)b->len;
+  *top = ta > tb ? ta : tb;
+  *bot = a->exp < b->exp ? a->exp : b->exp;
+  int64_t tl = *top - *bot;
+  if (p == 0) p = (size_t)tl;
+  else p += BIGFLOAT_EXTRA_PRECISION;
+  if (tl > (int64_t)p) *bot = *top - (int64_t)p;
+  return *top - (int64_t)p;
+}
+
+static void uadd(bigfloat_t t, const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p) {
+  int64_t bot, top;
+  int64_t e = window(a, b, p, &bot, &top);
+  size_t n = (size_t)(top - bot);
+  uint32_t *c = (uint32_t *)bc_xmalloc((n + 1) * sizeof(uint32_t));
+  uint64_t carry = 0;
+  for (size_t i = 0; i < n; i++) {
+    uint64_t w = (uint64_t)limb_at(a, bot + (int64_t)i) + limb_at(b, bot + (int64_t)i) + carry;
+    c[i] = (uint32_t)w;
+    carry = w >> 32;
+  }
+  if (carry) c[n++] = 1;
+  int sign = a->sign;
+  free(t->coef);
+  t->coef = c;
+  t->sign = sign;
+  t->exp = e;
+  t->len = n;
+}
+
+/* |a| >= |b| assumed (callers order the operands). */
+static void usub(bigfloat_t t, const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p) {
+  int64_t bot, top;
+  int64_t e = window(a, b, p, &bot, &top);
+  size_t n = (size_t)(top - bot);
+  uint32_t *c = (uint32_t *)bc_xmalloc((n + 1) * sizeof(uint32_t));
+  int64_t borrow = 0;
+  for (size_t i = 0; i < n; i++) {
+    int64_t w = (int64_t)limb_at(a, bot + (int64_t)i) - (int64_t)limb_at(b, bot + (int64_t)i) - borrow;
+    borrow = w < 0;
+    c[i] = (uint32_t)(w + (borrow ? ((int64_t)1 << 32) : 0));
+  }
+  while (n > 0 && c[n - 1] == 0) n--;
+  int sign = a->sign;
+  free(t->coef);
+  t->coef = c;
+  t->sign = sign;
+  t->exp = e;
+  t->len = n;
+  if (n == 0) bigfloat_zero(t);
+}
+
+/* bigfloat/addsub.c:183-210 */
+void bigfloat_add(bigfloat_t t, const bigfloat_t a, const bigfloat_t b, size_t p) {
+  if (a->sign == b->sign) {
+    uadd(t, a, b, p);
+  } else if (ucmp(a, b) > 0) {
+    usub(t, a, b, p);
+  } else {
+    usub(t, b, a, p);
+    bigfloat_neg(t);
+  }
+}
+
+/* bigfloat/addsub.c:212-237 */
+void bigfloat_sub(bigfloat_t t, const bigfloat_t a, const bigfloat_t b, size_t p) {
+  if (a->sign != b->sign) {
+    uadd(t, a, b, p);
+  } else if (ucmp(a, b) > 0) {
+    usub(t, a, b, p);
+  } else {
+    usub(t, b, a, p);
+    bigfloat_neg(t);
+  }
+}
+
+/* ---------------------------------------------------------------- multiply */
+
+/* Product length and trimming rule of bigfloat/mul.c:664-675. */
+static void trim_product(bigfloat_t t) {
+  if (t->coef[t->len - 1] == 0) t->len--;
+  if (t->len > 1000)
+    while (t->coef[t->len - 1] == 0) t->len--;
+}
+
+/* Operands after the precision chop of bigfloat/mul.c:573-602. */
+void bc_mul_operands(const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p, bc_operand *oa, bc_operand *ob) {
+  if (p == 0) p = a->len + b->len;
+  else p += BIGFLOAT_EXTRA_PRECISION;
+  oa->T = a->coef; oa->L = a->len; oa->exp = a->exp;
+  ob->T = b->coef; ob->L = b->len; ob->exp = b->exp;
+  if (oa->L > p) { size_t chop = oa->L - p; oa->L = p; oa->exp += (int64_t)chop; oa->T += chop; }
+  if (ob->L > p) { size_t chop = ob->L - p; ob->L = p; ob->exp += (int64_t)chop; ob->T += chop; }
+}
+
+/* bigfloat/mul.c:555-676: exact product of the chopped operands.  CL == 2 and
+ * CL < 100 stay on the host (the reference's fast path and Karatzuba range);
+ * everything else is one GPU product. */
+void bigfloat_mul(bigfloat_t t, const bigfloat_t a, const bigfloat_t b, size_t p) {
+  if (bigfloat_iszero(a) || bigfloat_iszero(b)) {
+    bigfloat_zero(t);
+    return;
+  }
+  bc_operand oa, ob;
+  bc_mul_operands(a, b, p, &oa, &ob);
+  const size_t CL = oa.L + ob.L;
+  const int sign = a->sign == b->sign;
+  const int64_t exp = oa.exp + ob.exp;
+  uint32_t *c = (uint32_t *)bc_xmalloc(CL * sizeof(uint32_t));
+  if (CL == 2) {
+    uint64_t r = (uint64_t)oa.T[0] * ob.T[0];
+    c[0] = (uint32_t)r;
+    c[1] = (uint32_t)(r >> 32);
+  } else if (CL < BC_SMALL_PRODUCT_LIMBS) {
+    bc_small_mul(c, CL, oa.T, oa.L, ob.T, ob.L);
+  } else {
+    _fft_mul(c, CL, (uint32_t *)oa.T, oa.L, (uint32_t *)ob.T, ob.L);
+  }
+  free(t->coef);
+  t->coef = c;
+  t->sign = sign;
+  t->exp = exp;
+  t->len = CL;
+  trim_product(t);
+}
+
+/* Batch of bigfloat_mul: small products on the host, the rest in one
+ * bc_gpu_mul_batch call.  Each result is what bigfloat_mul would produce. */
+void bigfloat_mul_batch(bigfloat_mul_item *items, size_t n) {
+  bc_gpu_item *g = (bc_gpu_item *)bc_xmalloc((n ? n : 1) * sizeof(bc_gpu_item));
+  size_t ng = 0;
+  for (size_t i = 0; i < n; i++) {
+    _bigfloat_struct *t = items[i].target;
+    const _bigfloat_struct *a = items[i].a, *b = items[i].b;
+    if (bigfloat_iszero(a) || bigfloat_iszero(b)) {
+      bigfloat_zero(t);
+      continue;
+    }
+    bc_operand oa, ob;
+    bc_mul_operands(a, b, items[i].p, &oa, &ob);
+    const size_t CL = oa.L + ob.L;
+    uint32_t *c = (uint32_t *)bc_xmalloc(CL * sizeof(uint32_t));
+    if (CL == 2) {
+      uint64_t r = (uint64_t)oa.T[0] * ob.T[0];
+      c[0] = (uint32_t)r;
+      c[1] = (uint32_t)(r >> 32);
+    } else if (CL < BC_SMALL_PRODUCT_LIMBS) {
+      bc_small_mul(c, CL, oa.T, oa.L, ob.T, ob.L);
+    } else {
+      g[ng].C = c; g[ng].CL = CL; g[ng].A = oa.T; g[ng].AL = oa.L; g[ng].B = ob.T; g[ng].BL = ob.L;
+      ng++;
+    }
+    /* fields are set now; the limbs of GPU items arrive below */
+    free(t->coef);
+    t->coef = c;
+    t->sign = a->sign == b->sign;
+    t->exp = oa.exp + ob.exp;
+    t->len = CL;
+  }
+  if (ng) bc_host_gpu_batch(g, ng);
+  for (size_t i = 0; i < n; i++)
+    if (items[i].target->len) trim_product(items[i].target);
+  free(g);
+}
+
+/* bigfloat/mul.c:64-80: a *= b in place over a->len limbs, the top limb
+ * cleared first and the final carry dropped. */
+void bigfloat_mului(bigfloat_t a, uint32_t b) {
+  a->coef[a->len - 1] = 0;
+  uint64_t carry = 0;
+  for (size_t i = 0; i < a->len; i++) {
+    uint64_t v = (uint64_t)a->coef[i] * b + carry;
+    a->coef[i] = (uint32_t)v;
+    carry = v >> 32;
+  }
+}
+
+/* bigfloat/mul.c:83-102: target->len limbs of a*b (target allocated by the
+ * caller, final carry dropped). */
+void bigfloat_mulu(bigfloat_t t, const bigfloat_t a, uint32_t b) {
+  uint64_t carry = 0;
+  for (size_t i = 0; i < t->len; i++) {
+    uint64_t v = carry;
+    if (i < a->len) v += (uint64_t)a->coef[i] * b;
+    t->coef[i] = (uint32_t)v;
+    carry = v >> 32;
+  }
+}
+
+/* bigfloat/exp.c:13-29: square and multiply, in place, no truncation. */
+void bigfloat_exp(bigfloat_t t, const bigfloat_t a, uint64_t e) {
+  bigfloat_t cp;
+  bigfloat_new(cp);
+  bigfloat_copy(cp, a);
+  bigfloat_set(t, 1);
+  while (e > 0) {
+    if (e % 2 == 1) bigfloat_mul(t, t, cp, 0);
+    bigfloat_mul(cp, cp, cp, 0);
+    e /= 2;
+  }
+  bigfloat_free(cp);
+}

@@ -1,0 +1,223 @@
+/* e.c — e = sum 1/k! to N decimal digits (the reference's main.c:38-167).
+ *
+ * Binary splitting P(a,b), Q(a,b): leaves P = 1, Q = b; a node combines its
+ * halves (split at m = (a+b)/2) as P = P0*Q1 + P1, Q = Q0*Q1
+ * (main.c:63-109).  Then e = 1 + P/Q by Newton division at p limbs
+ * (main.c:131-140), hex output, radix conversion and decimal output
+ * (main.c:143-166).
+ *
+ * Two drivers for the splitting tree, same values:
+ *   mode 0  the reference's recursion, one product per GPU call;
+ *   mode 1  level order: subtrees of at most LEAF_TERMS terms run the same
+ *           recursion on host threads (all their products are below 100
+ *           limbs, the reference's host range), and every level above them
+ *           multiplies all of its 2*nodes products in one bigfloat_mul_batch.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "bc_host.h"
+#include "bench.h"
+#include "bigfloat.h"
+
+/* main.c:38-61: terms so that log(terms!) exceeds p limbs of precision. */
+static size_t e_terms(size_t p) {
+  long double sizeL = (long double)p * logl(4294967296.0L) + 1;
+  size_t a = 0, b = 1;
+  while (lgammal((long double)b) < sizeL) b *= 2;
+  while (b - a > 1) {
+    size_t m = (a + b) / 2;
+    if (lgammal((long double)m) < sizeL) a = m;
+    else b = m;
+  }
+  return b + 2;
+}
+
+/* main.c:63-109 without the DEBUG timers. */
+static void bsr(bigfloat_t P, bigfloat_t Q, uint32_t a, uint32_t b) {
+  if (b - a == 1) {
+    bigfloat_set(P, 1);
+    bigfloat_set(Q, b);
+    return;
+  }
+  uint32_t m = (a + b) / 2;
+  bigfloat_t P0, Q0, P1, Q1, t;
+  bigfloat_new(P0); bigfloat_new(Q0); bigfloat_new(P1); bigfloat_new(Q1); bigfloat_new(t);
+  bsr(P0, Q0, a, m);
+  bsr(P1, Q1, m, b);
+  bigfloat_mul(t, P0, Q1, 0);
+  bigfloat_free(P0);
+  bigfloat_add(P, t, P1, 0);
+  bigfloat_free(t);
+  bigfloat_free(P1);
+  bigfloat_mul(Q, Q0, Q1, 0);
+  bigfloat_free(Q1);
+  bigfloat_free(Q0);
+}
+
+/* Subtrees of this many terms or fewer stay on host threads: their P and Q
+ * stay below 64 limbs for up to 2^32 terms, so every product is < 100 limbs. */
+#define LEAF_TERMS 64
+
+typedef struct {
+  uint32_t a, b;
+  int c0, c1;           /* children in the next level, -1 if computed on the host */
+  _bigfloat_struct P, Q;
+} bnode;
+
+static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
+  /* top-down: the tree above the host subtrees, one array per depth */
+  bnode **lv = (bnode **)bc_xmalloc(sizeof(bnode *));
+  size_t *cnt = (size_t *)bc_xmalloc(sizeof(size_t));
+  lv[0] = (bnode *)calloc(1, sizeof(bnode));
+  lv[0][0].a = a0;
+  lv[0][0].b = b0;
+  cnt[0] = 1;
+  int nlv = 1;
+  for (;;) {
+    bnode *L = lv[nlv - 1];
+    size_t m = cnt[nlv - 1], nin = 0;
+    for (size_t i = 0; i < m; i++) nin += (L[i].b - L[i].a) > LEAF_TERMS;
+    if (!nin) break;
+    bnode *N = (bnode *)calloc(2 * nin, sizeof(bnode));
+    size_t c = 0;
+    for (size_t i = 0; i < m; i++) {
+      bnode *x = &L[i];
+      x->c0 = x->c1 = -1;
+      if (x->b - x->a <= LEAF_TERMS) continue;
+      uint32_t mid = (x->a + x->b) / 2;
+      N[c].a = x->a; N[c].b = mid; x->c0 = (int)c++;
+      N[c].a = mid; N[c].b = x->b; x->c1 = (int)c++;
+    }
+    lv = (bnode **)bc_xrealloc(lv, (size_t)(nlv + 1) * sizeof(bnode *));
+    cnt = (size_t *)bc_xrealloc(cnt, (size_t)(nlv + 1) * sizeof(size_t));
+    lv[nlv] = N;
+    cnt[nlv] = c;
+    nlv++;
+  }
+  /* host subtrees (every level may hold some), in parallel */
+  for (int d = 0; d < nlv; d++) {
+    bnode *L = lv[d];
+    long m = (long)cnt[d];
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long i = 0; i < m; i++) {
+      bnode *x = &L[i];
+      if (x->b - x->a > LEAF_TERMS) continue;
+      bigfloat_new(&x->P);
+      bigfloat_new(&x->Q);
+      bsr(&x->P, &x->Q, x->a, x->b);
+    }
+  }
+  /* bottom-up: one batch of 2 products per internal node, then the adds */
+  for (int d = nlv - 2; d >= 0; d--) {
+    bnode *L = lv[d], *N = lv[d + 1];
+    size_t m = cnt[d], q = 0;
+    for (size_t i = 0; i < m; i++) q += L[i].c0 >= 0;
+    bigfloat_mul_item *it = (bigfloat_mul_item *)bc_xmalloc(2 * q * sizeof(bigfloat_mul_item));
+    _bigfloat_struct *tmp = (_bigfloat_struct *)calloc(q ? q : 1, sizeof(_bigfloat_struct));
+    size_t j = 0;
+    for (size_t i = 0; i < m; i++) {
+      bnode *x = &L[i];
+      if (x->c0 < 0) continue;
+      bnode *l = &N[x->c0], *r = &N[x->c1];
+      bigfloat_new(&tmp[j / 2]);
+      bigfloat_new(&x->P);
+      bigfloat_new(&x->Q);
+      it[j].target = &tmp[j / 2]; it[j].a = &l->P; it[j].b = &r->Q; it[j].p = 0; j++;  /* P0*Q1 */
+      it[j].target = &x->Q;       it[j].a = &l->Q; it[j].b = &r->Q; it[j].p = 0; j++;  /* Q0*Q1 */
+    }
+    bigfloat_mul_batch(it, j);
+    free(it);
+    long mm = (long)m;
+    j = 0;
+    size_t *slot = (size_t *)bc_xmalloc((m ? m : 1) * sizeof(size_t));
+    for (size_t i = 0; i < m; i++) { slot[i] = j; j += L[i].c0 >= 0; }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long i = 0; i < mm; i++) {
+      bnode *x = &L[i];
+      if (x->c0 < 0) continue;
+      bnode *l = &N[x->c0], *r = &N[x->c1];
+      bigfloat_add(&x->P, &tmp[slot[i]], &r->P, 0);   /* P = P0*Q1 + P1 */
+      bigfloat_free(&tmp[slot[i]]);
+      bigfloat_free(&l->P); bigfloat_free(&l->Q); bigfloat_free(&r->P); bigfloat_free(&r->Q);
+    }
+    free(slot);
+    free(tmp);
+    free(N);
+  }
+  free(P->coef);
+  free(Q->coef);
+  *P = lv[0][0].P;
+  *Q = lv[0][0].Q;
+  free(lv[0]);
+  free(lv);
+  free(cnt);
+}
+
+static int dump(const char *dir, const char *name, const char *s, size_t len) {
+  char path[4096];
+  snprintf(path, sizeof path, "%s/%s", dir ? dir : ".", name);
+  FILE *f = fopen(path, "wb");
+  if (!f) {
+    fprintf(stderr, "Cannot create file %s\n", path);
+    return -1;
+  }
+  fwrite(s, 1, len, f);
+  fclose(f);
+  return 0;
+}
+
+/* main.c:111-167 */
+int bluecrunch_e(size_t digits, int mode, const char *outdir) {
+  digits++;  /* the leading 2 does not count */
+  size_t p = (digits + 8) / 9;
+  size_t terms = e_terms(p);
+  if ((uint32_t)terms != terms) {
+    fprintf(stderr, "Limit Exceeded");
+    return -1;
+  }
+  task_start(1, "Summing");
+  bigfloat_t P, Q;
+  bigfloat_new(P);
+  bigfloat_new(Q);
+  if (mode == 1) bsr_levels(P, Q, 0, (uint32_t)terms);
+  else bsr(P, Q, 0, (uint32_t)terms);
+  task_end(1);
+
+  task_start(1, "Dividing");
+  bigfloat_t one, tmp;
+  bigfloat_new(one);
+  bigfloat_set(one, 1);
+  bigfloat_new(tmp);
+  bigfloat_div(tmp, P, Q, p);
+  bigfloat_free(Q);
+  bigfloat_add(P, tmp, one, p);
+  bigfloat_free(tmp);
+  bigfloat_free(one);
+  task_end(1);
+
+  task_start(1, "Writing hex digits");
+  size_t out_len = digits + 2;
+  char *out = (char *)bc_xmalloc(out_len + 22);
+  size_t len = bigfloat_to_string(out, P, out_len, 16);
+  int rc = dump(outdir, "e-hex.txt", out, len);
+  task_end(1);
+
+  task_start(1, "Converting to decimal");
+  fflush(stdout);
+  bigfloat_t dec;
+  bigfloat_new(dec);
+  bigfloat_radix(dec, P);
+  task_end(1);
+
+  task_start(1, "Writing decimal digits");
+  len = bigfloat_to_string(out, dec, out_len, 10);
+  rc |= dump(outdir, "e.txt", out, len);
+  bigfloat_free(P);
+  bigfloat_free(dec);
+  free(out);
+  task_end(1);
+  return rc;
+}

@@ -1,0 +1,30 @@
+/* main.c — command line: bluecrunch <digits> [--per-call]
+ * Computes e to <digits> decimal digits into ./e.txt and ./e-hex.txt, like
+ * the reference's main.c:169-219; products run on the GPU.  --per-call uses
+ * the reference's recursion with one GPU product per call instead of the
+ * level-batched tree. */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "bench.h"
+#include "bigfloat.h"
+
+int main(int argc, char *argv[]) {
+  if (argc < 2) {
+    printf("Usage %s <number of digits> [--per-call] - Computes Eulers constant\n", argv[0]);
+    return 0;
+  }
+  size_t digits = strtoull(argv[1], NULL, 10);
+  int mode = 1;
+  for (int i = 2; i < argc; i++)
+    if (!strcmp(argv[i], "--per-call")) mode = 0;
+  printf("Configuration:\n");
+  printf("Digits:           %zu\n", digits);
+  printf("Multiply:         B200 FP64 FFT (%s)\n", mode ? "tree levels batched" : "one product per call");
+  printf("Output File:      ./e.txt\n\n");
+  task_start(0, "Starting calculation");
+  int rc = bluecrunch_e(digits, mode, NULL);
+  task_end(0);
+  return rc ? 1 : 0;
+}

@@ -1,0 +1,169 @@
+/* mul_shim.c — the reference's multiply entry points (include/mul.h) on top
+ * of libbcgpu.
+ *
+ * _fft_mul keeps the prototype of bigfloat/mul.c:108 and its contract
+ * (exactly CL limbs of A*B mod 2^(32 CL), CT may alias AT or BT, no status
+ * return) but runs on the GPU.  The engine is initialised on first use; a
+ * failure is reported on stderr and aborts, as the reference aborts on the
+ * widths it cannot handle (fft/convert.c:66-68).  There is no CPU fallback.
+ */
+#define _GNU_SOURCE
+#include <dlfcn.h>
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "bc_gpu.h"
+#include "bc_host.h"
+#include "bigfloat.h"
+#include "mul.h"
+
+static pthread_once_t g_once = PTHREAD_ONCE_INIT;
+static int g_init_rc = 0;
+static bigfloat_mul_counters g_cnt;
+static pthread_mutex_t g_cnt_mu = PTHREAD_MUTEX_INITIALIZER;
+
+void *bc_xmalloc(size_t n) {
+  void *p = malloc(n ? n : 1);
+  if (!p) {
+    fprintf(stderr, "bluecrunch: out of host memory (%zu bytes)\n", n);
+    abort();
+  }
+  return p;
+}
+
+void *bc_xrealloc(void *p, size_t n) {
+  void *q = realloc(p, n ? n : 1);
+  if (!q) {
+    fprintf(stderr, "bluecrunch: out of host memory (%zu bytes)\n", n);
+    abort();
+  }
+  return q;
+}
+
+static double now_s(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * t.tv_nsec;
+}
+
+/* Width table: $BC_TUNE_FILE, else tune/widths.txt next to this library. */
+static void init_once(void) {
+  static char path[4096];
+  bc_gpu_config cfg;
+  memset(&cfg, 0, sizeof cfg);
+  const char *env = getenv("BC_TUNE_FILE");
+  if (env) {
+    cfg.tune_path = env;
+  } else {
+    Dl_info info;
+    if (dladdr((void *)&init_once, &info) && info.dli_fname) {
+      snprintf(path, sizeof path, "%s", info.dli_fname);
+      char *slash = strrchr(path, '/');
+      if (slash) {
+        snprintf(slash + 1, sizeof path - (size_t)(slash + 1 - path), "tune/widths.txt");
+        cfg.tune_path = path;
+      }
+    }
+  }
+  const char *dev = getenv("BC_DEVICE");
+  cfg.device = dev ? atoi(dev) : 0;
+  g_init_rc = bc_gpu_init(&cfg);
+}
+
+static void ensure_gpu(void) {
+  pthread_once(&g_once, init_once);
+  if (g_init_rc != BC_OK) {
+    fprintf(stderr, "bluecrunch: GPU engine unavailable: %s\n", bc_gpu_strerror(g_init_rc));
+    abort();
+  }
+}
+
+static void count(size_t products, size_t calls, double secs) {
+  pthread_mutex_lock(&g_cnt_mu);
+  g_cnt.gpu_products += products;
+  g_cnt.gpu_calls += calls;
+  g_cnt.gpu_seconds += secs;
+  pthread_mutex_unlock(&g_cnt_mu);
+}
+
+int _fft_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *BT, size_t BL) {
+  ensure_gpu();
+  bc_mul_stats st;
+  double t0 = now_s();
+  int rc = bc_gpu_mul(CT, CL, AT, AL, BT, BL, &st);
+  count(1, 1, now_s() - t0);
+  if (rc != BC_OK) {
+    fprintf(stderr, "_fft_mul: GPU multiply failed (CL=%zu): %s\n", CL, bc_gpu_strerror(rc));
+    abort();
+  }
+  return st.width;
+}
+
+void bc_host_gpu_batch(bc_gpu_item *items, size_t n) {
+  ensure_gpu();
+  bc_mul_desc *d = (bc_mul_desc *)bc_xmalloc(n * sizeof(bc_mul_desc));
+  for (size_t i = 0; i < n; i++) {
+    d[i].C = items[i].C; d[i].CL = items[i].CL;
+    d[i].A = items[i].A; d[i].AL = items[i].AL;
+    d[i].B = items[i].B; d[i].BL = items[i].BL;
+  }
+  bc_batch_stats st;
+  double t0 = now_s();
+  int rc = bc_gpu_mul_batch(d, n, &st);
+  count(n, 1, now_s() - t0);
+  free(d);
+  if (rc != BC_OK) {
+    fprintf(stderr, "bigfloat_mul_batch: GPU batch of %zu products failed: %s\n", n, bc_gpu_strerror(rc));
+    abort();
+  }
+}
+
+/* Exact schoolbook product of the low CL limbs (the value the reference's
+ * _basecase_mul, bigfloat/mul.c:176-220, and _karatzuba_mul, :367-553,
+ * produce).  Works through a temporary so CT may alias AT or BT. */
+void bc_small_mul(uint32_t *CT, size_t CL, const uint32_t *AT, size_t AL, const uint32_t *BT, size_t BL) {
+  uint32_t stackbuf[256];
+  uint32_t *P = CL <= 256 ? stackbuf : (uint32_t *)bc_xmalloc(CL * sizeof(uint32_t));
+  memset(P, 0, CL * sizeof(uint32_t));
+  for (size_t i = 0; i < AL && i < CL; i++) {
+    uint64_t carry = 0;
+    const uint64_t ai = AT[i];
+    size_t j = 0;
+    for (; j < BL && i + j < CL; j++) {
+      uint64_t v = (uint64_t)P[i + j] + ai * BT[j] + carry;
+      P[i + j] = (uint32_t)v;
+      carry = v >> 32;
+    }
+    for (size_t k = i + j; k < CL && carry; k++) {
+      uint64_t v = (uint64_t)P[k] + carry;
+      P[k] = (uint32_t)v;
+      carry = v >> 32;
+    }
+  }
+  memcpy(CT, P, CL * sizeof(uint32_t));
+  if (P != stackbuf) free(P);
+  __atomic_add_fetch(&g_cnt.small_products, 1, __ATOMIC_RELAXED);
+}
+
+void _basecase_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *BT, size_t BL) {
+  bc_small_mul(CT, CL, AT, AL, BT, BL);
+}
+
+void _karatzuba_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *BT, size_t BL) {
+  bc_small_mul(CT, CL, AT, AL, BT, BL);
+}
+
+void bigfloat_get_counters(bigfloat_mul_counters *out) {
+  pthread_mutex_lock(&g_cnt_mu);
+  *out = g_cnt;
+  pthread_mutex_unlock(&g_cnt_mu);
+}
+
+void bigfloat_reset_counters(void) {
+  pthread_mutex_lock(&g_cnt_mu);
+  memset(&g_cnt, 0, sizeof g_cnt);
+  pthread_mutex_unlock(&g_cnt_mu);
+}

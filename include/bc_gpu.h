@@ -111,6 +111,10 @@ int bc_gpu_set_width_limit(size_t fft_points, int width);
 
 /* Force the width of subsequent products (0 = automatic); for error sweeps. */
 int bc_gpu_force_width(int width);
+/* Supported transform lengths in increasing order; returns the count. */
+int bc_gpu_lengths(size_t *out, int cap);
+/* Force transform length and width (0, 0 = automatic); for the autotuner. */
+int bc_gpu_force_plan(size_t fft_points, int width);
 
 int bc_gpu_sync(void);
 int bc_gpu_last_error(void);
