@@ -82,6 +82,7 @@ GPU_SYMBOLS = {
     "bc_gpu_force_width": (ctypes.c_int, [ctypes.c_int]),
     "bc_gpu_force_plan": (ctypes.c_int, [_sz, ctypes.c_int]),
     "bc_gpu_lengths": (ctypes.c_int, [ctypes.POINTER(_sz), ctypes.c_int]),
+    "bc_gpu_load_width_table": (ctypes.c_int, [ctypes.c_char_p]),
     "bc_gpu_sync": (ctypes.c_int, []),
     "bc_gpu_last_error": (ctypes.c_int, []),
     "bc_gpu_last_cuda_error": (ctypes.c_int, []),
@@ -114,9 +115,11 @@ def _check(code, what=""):
 
 
 def init(device=0, arena_bytes=0, tune_path=None, max_round_err=0.25, verbose=0):
+    global _widths_loaded
     if tune_path is None:
         default = os.path.join(PKG, "tune", "widths.txt")
         tune_path = default if os.path.exists(default) else None
+    _widths_loaded = bool(tune_path)
     cfg = Config(device, arena_bytes, tune_path.encode() if tune_path else None, max_round_err, verbose)
     _check(_lib().bc_gpu_init(ctypes.byref(cfg)), "bc_gpu_init")
 
@@ -185,7 +188,20 @@ def mul_batch_desc(descs, n):
     return {k: getattr(st, k) for k, _ in BatchStats._fields_}
 
 
+TUNE_FILE = os.path.join(PKG, "tune", "widths.txt")
+_widths_loaded = False
+
+
+def load_width_table(path=TUNE_FILE):
+    """Load the tuned width table into the library (no GPU needed)."""
+    global _widths_loaded
+    _check(_lib().bc_gpu_load_width_table(path.encode()), "bc_gpu_load_width_table")
+    _widths_loaded = True
+
+
 def plan(AL, BL, CL=None, square=False):
+    if not _widths_loaded and os.path.exists(TUNE_FILE):
+        load_width_table()
     info = PlanInfo()
     _check(_lib().bc_gpu_plan(AL, BL, CL or (AL + BL), int(square), ctypes.byref(info)), "bc_gpu_plan")
     return {k: getattr(info, k) for k, _ in PlanInfo._fields_}

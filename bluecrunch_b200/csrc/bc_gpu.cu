@@ -876,6 +876,17 @@ int bc_gpu_force_width(int width) {
   return BC_OK;
 }
 
+int bc_gpu_load_width_table(const char *path) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!path) return BC_ERR_INVALID;
+  FILE *f = fopen(path, "r");
+  if (!f) return BC_ERR_INVALID;
+  fclose(f);
+  g.width_file.clear();
+  load_width_file(path);
+  return BC_OK;
+}
+
 int bc_gpu_lengths(size_t *out, int cap) {
   const std::vector<size_t> &v = lengths();
   for (int i = 0; i < cap && i < (int)v.size(); i++) out[i] = v[i];

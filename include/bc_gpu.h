@@ -104,6 +104,9 @@ int bc_gpu_set_stream(void *stream);
 
 int bc_gpu_plan(size_t AL, size_t BL, size_t CL, int square, bc_plan_info *out);
 
+/* Load a width table (lines "M width"); no GPU needed.  bc_gpu_init loads
+ * bc_gpu_config.tune_path or $BC_TUNE_FILE itself. */
+int bc_gpu_load_width_table(const char *path);
 /* Largest width allowed at transform length M by the loaded width table. */
 int bc_gpu_width_limit(size_t fft_points);
 /* Override the width limit for one transform length (autotuner); 0 = reset. */

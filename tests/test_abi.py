@@ -1,0 +1,72 @@
+"""CPU: the C-ABI libraries load and export every declared symbol; planning
+and width logic (no GPU calls)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import bluecrunch_b200 as bc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\([^;{]*\)\s*;", text, re.M))
+
+
+def test_gpu_library_exports_header():
+    names = _declared("bc_gpu.h")
+    assert "bc_gpu_mul" in names and "bc_gpu_mul_batch" in names
+    lib = ctypes.CDLL(bc.GPU_LIB)
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(bc.GPU_SYMBOLS) >= names
+
+
+def test_host_library_exports_reference_prototypes():
+    lib = ctypes.CDLL(bc.HOST_LIB)
+    for header in ("bigfloat.h", "mul.h", "bench.h"):
+        for n in _declared(header):
+            assert hasattr(lib, n), (header, n)
+
+
+def test_strerror_and_uninitialised_calls():
+    lib = bc._lib()
+    for code in range(0, -10, -1):
+        assert lib.bc_gpu_strerror(code)
+    # nothing initialised in this process: calls report, never abort
+    assert lib.bc_gpu_sync() in (bc.BC_OK, -6)
+
+
+@pytest.mark.parametrize("n", [1, 50, 100, 999, 4096, 10**5, 2**20, 3 * 2**20 + 5, 2**26])
+def test_plans_fit_and_are_exact_sized(n):
+    for (al, bl) in [(n, n), (n, max(1, n // 8)), (n, 1)]:
+        p = bc.plan(al, bl)
+        M, b = p["fft_points"], p["width"]
+        assert 8 <= b <= 24
+        assert p["digits_a"] == -(-32 * al // b) and p["digits_b"] == -(-32 * bl // b)
+        # acyclic product must fit the 2M real coefficients
+        assert p["digits_a"] + p["digits_b"] - 1 <= 2 * M
+        assert b <= bc.width_limit(M)
+        assert p["levels"] in (1, 2, 3)
+        assert p["L1"] * p["L2"] * max(p["Lr"], 1) == M
+
+
+def test_lengths_are_2k_or_3x2k():
+    L = bc.lengths()
+    assert L == sorted(L) and L[0] == 256 and L[-1] == 1 << 30
+    for M in L:
+        m = M // 3 if M % 3 == 0 else M
+        assert m & (m - 1) == 0
+
+
+def test_width_table_monotone():
+    bc.load_width_table()
+    prev = 99
+    for M in bc.lengths():
+        w = bc.width_limit(M)
+        assert w <= prev + 1  # non-increasing up to one-step noise
+        prev = w

@@ -1,0 +1,115 @@
+"""CPU: the host C library (include/bigfloat.h) on sizes whose products all
+stay below 100 limbs, where bigfloat_mul never calls the GPU (the reference's
+own host range, bigfloat/mul.c:640-648)."""
+import ctypes
+import hashlib
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import bluecrunch_b200 as bc
+import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run_e(digits, tmp, per_call=False):
+    cmd = [bc.CLI, str(digits)] + (["--per-call"] if per_call else [])
+    subprocess.run(cmd, cwd=tmp, check=True, stdout=subprocess.DEVNULL, timeout=120)
+    return open(os.path.join(tmp, "e.txt"), "rb").read(), open(os.path.join(tmp, "e-hex.txt"), "rb").read()
+
+
+@pytest.mark.parametrize("digits", [10, 50, 100, 200, 250, 400])
+def test_e_small_matches_true_digits(digits):
+    import mpmath
+    mpmath.mp.dps = digits + 30
+    want = mpmath.nstr(mpmath.e, digits + 10, strip_zeros=False)
+    with tempfile.TemporaryDirectory() as d:
+        dec, hexs = _run_e(digits, d)
+        dec2, hex2 = _run_e(digits, d, per_call=True)
+    assert want.startswith(dec.decode())
+    if digits >= 50:  # below that the output stops at a whole limb, as the reference's does
+        assert len(dec) == digits + 2
+    assert (dec, hexs) == (dec2, hex2)
+
+
+@pytest.mark.parametrize("digits", [50, 100, 200, 400])
+def test_e_small_matches_reference_build(digits):
+    if not os.path.exists(oracle.reference_cli("serial")):
+        pytest.skip("reference build not present")
+    with tempfile.TemporaryDirectory() as d:
+        mine = _run_e(digits, d)
+        subprocess.run([oracle.reference_cli("serial"), str(digits)], cwd=d, check=True,
+                       stdout=subprocess.DEVNULL)
+        ref = (open(os.path.join(d, "e.txt"), "rb").read(), open(os.path.join(d, "e-hex.txt"), "rb").read())
+    assert mine == ref
+
+
+class BF(ctypes.Structure):
+    _fields_ = [("coef", ctypes.POINTER(ctypes.c_uint32)), ("exp", ctypes.c_int64),
+                ("len", ctypes.c_size_t), ("sign", ctypes.c_int)]
+
+
+def _host():
+    lib = ctypes.CDLL(bc.HOST_LIB)
+    P = ctypes.POINTER(BF)
+    for n in ("bigfloat_new", "bigfloat_free", "bigfloat_zero"):
+        getattr(lib, n).argtypes = [P]
+    lib.bigfloat_set.argtypes = [P, ctypes.c_uint32]
+    lib.bigfloat_exp.argtypes = [P, P, ctypes.c_uint64]
+    lib.bigfloat_mul.argtypes = [P, P, P, ctypes.c_size_t]
+    lib.bigfloat_add.argtypes = [P, P, P, ctypes.c_size_t]
+    lib.bigfloat_sub.argtypes = [P, P, P, ctypes.c_size_t]
+    lib.bigfloat_radix.argtypes = [P, P]
+    return lib
+
+
+def _val(x):
+    return int.from_bytes(np.ctypeslib.as_array(x.coef, (x.len,)).astype("<u4").tobytes(), "little") if x.len else 0
+
+
+def test_power_known_answer():
+    # test/test_bigfloat_exp.c: 0x1234^0xd7 has 82 limbs (all products < 100 limbs)
+    lib = _host()
+    a, b = BF(), BF()
+    lib.bigfloat_new(a); lib.bigfloat_new(b)
+    lib.bigfloat_set(a, 0x1234)
+    lib.bigfloat_exp(b, a, 0xD7)
+    assert b.len == 82 and b.exp == 0 and b.sign == 1
+    assert _val(b) == 0x1234 ** 0xD7
+
+
+def test_in_place_square_regression():
+    # test/test_regression.c:40-67: bigfloat_mul(a, a, a, 0) in place
+    lib = _host()
+    a = BF()
+    lib.bigfloat_new(a)
+    arr = (ctypes.c_uint32 * 4)(0x44210000, 0xb1514c28, 0xce88deb8, 0x2)
+    lib.bigfloat_set(a, 1)
+    libc = ctypes.CDLL(None)
+    libc.malloc.restype = ctypes.c_void_p
+    mem = libc.malloc(16)
+    ctypes.memmove(mem, arr, 16)
+    a.coef = ctypes.cast(mem, ctypes.POINTER(ctypes.c_uint32))
+    a.len, a.exp, a.sign = 4, 0, 1
+    lib.bigfloat_mul(a, a, a, 0)
+    got = list(np.ctypeslib.as_array(a.coef, (a.len,)))
+    assert got == [0x0, 0xf4718c41, 0x21c8adaa, 0x28b6543c, 0x68a5465b, 0xe0c40a81, 0x7]
+
+
+def test_add_sub_truncation_semantics():
+    # precision p keeps p+2 limbs (bigfloat/addsub.c:83-86): exponent top-(p+2)
+    lib = _host()
+    x, y, t = BF(), BF(), BF()
+    for z in (x, y, t):
+        lib.bigfloat_new(z)
+    lib.bigfloat_set(x, 7)
+    lib.bigfloat_set(y, 5)
+    y.exp = -10
+    lib.bigfloat_add(t, x, y, 3)
+    assert t.len == 5 and t.exp == 1 - 5 and _val(t) == 7 << (32 * 4)
+    lib.bigfloat_sub(t, x, y, 0)
+    assert t.exp == -10 and t.len == 11 and t.sign == 1
