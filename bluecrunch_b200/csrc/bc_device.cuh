@@ -299,16 +299,16 @@ struct RunRec {
 // delta_r out of H_r + X_r beyond C_{r-1} is in {-1,0,1}.  The map
 // delta_{r-1} -> delta_r is kept as three 2-bit fields (value+1) for inputs
 // -1, 0, +1; composition gives a scan.
-__device__ __forceinline__ int fn_apply(uint32_t f, int d) { return (int)((f >> (2 * (d + 1))) & 3) - 1; }
-__device__ __forceinline__ uint32_t fn_make(int vm, int v0, int vp) {
+__host__ __device__ __forceinline__ int fn_apply(uint32_t f, int d) { return (int)((f >> (2 * (d + 1))) & 3) - 1; }
+__host__ __device__ __forceinline__ uint32_t fn_make(int vm, int v0, int vp) {
   return (uint32_t)(vm + 1) | ((uint32_t)(v0 + 1) << 2) | ((uint32_t)(vp + 1) << 4);
 }
 constexpr uint32_t FN_ID = 0u | (1u << 2) | (2u << 4);
-__device__ __forceinline__ bool fn_is_const(uint32_t f) {
+__host__ __device__ __forceinline__ bool fn_is_const(uint32_t f) {
   return (f & 3u) == ((f >> 2) & 3u) && (f & 3u) == ((f >> 4) & 3u);
 }
 // result = second(first(x))
-__device__ __forceinline__ uint32_t fn_compose(uint32_t first, uint32_t second) {
+__host__ __device__ __forceinline__ uint32_t fn_compose(uint32_t first, uint32_t second) {
   return fn_make(fn_apply(second, fn_apply(first, -1)), fn_apply(second, fn_apply(first, 0)),
                  fn_apply(second, fn_apply(first, 1)));
 }
@@ -317,7 +317,7 @@ __device__ __forceinline__ uint32_t fn_compose(uint32_t first, uint32_t second) 
 struct U192 { unsigned long long w[3]; };
 
 // H + v (v signed 64-bit) modulo 2^nbits; returns the carry out in {-1,0,1}.
-__device__ __forceinline__ int u192_add_s64(U192 &h, long long v, int nbits) {
+__host__ __device__ __forceinline__ int u192_add_s64(U192 &h, long long v, int nbits) {
   unsigned long long add = (unsigned long long)v;
   unsigned long long ext = v < 0 ? ~0ull : 0ull;
   unsigned long long s0 = h.w[0] + add;
@@ -352,14 +352,14 @@ __device__ __forceinline__ int u192_add_s64(U192 &h, long long v, int nbits) {
       if (bi == 0) { h.w[1] = 0; h.w[2] = 0; }
       else { h.w[1] &= (1ull << bi) - 1; h.w[2] = 0; }
     } else {
-      if (bi != 0) h.w[2] &= (1ull << bi) - 1;
+      h.w[2] = bi ? (h.w[2] & ((1ull << bi) - 1)) : 0;
     }
   }
   return carry;
 }
 
-__device__ __forceinline__ bool u192_is_zero(const U192 &h) { return (h.w[0] | h.w[1] | h.w[2]) == 0; }
-__device__ __forceinline__ bool u192_is_ones(const U192 &h, int nbits) {
+__host__ __device__ __forceinline__ bool u192_is_zero(const U192 &h) { return (h.w[0] | h.w[1] | h.w[2]) == 0; }
+__host__ __device__ __forceinline__ bool u192_is_ones(const U192 &h, int nbits) {
   const int wi = nbits >> 6, bi = nbits & 63;
   unsigned long long m2 = 0, m1 = ~0ull;
   if (wi == 1) { m1 = bi ? ((1ull << bi) - 1) : 0; m2 = 0; }
@@ -370,7 +370,7 @@ __device__ __forceinline__ bool u192_is_ones(const U192 &h, int nbits) {
 }
 
 // Bits [off, off+32) of a 192-bit value (off may exceed 192 -> 0).
-__device__ __forceinline__ uint32_t u192_bits32(const U192 &h, int off) {
+__host__ __device__ __forceinline__ uint32_t u192_bits32(const U192 &h, int off) {
   if (off >= 192) return 0;
   const int wi = off >> 6, bi = off & 63;
   unsigned long long lo = h.w[wi] >> bi;
@@ -380,14 +380,14 @@ __device__ __forceinline__ uint32_t u192_bits32(const U192 &h, int off) {
 
 // Map for one run: given H_r (8b bits) and C_{r-1}, produce H'_r, G_r and
 // the transfer function delta_{r-1} -> delta_r.
-__device__ __forceinline__ uint32_t run_transfer(U192 &h, long long cprev, int nbits) {
+__host__ __device__ __forceinline__ uint32_t run_transfer(U192 &h, long long cprev, int nbits) {
   int g = u192_add_s64(h, cprev, nbits);
   bool z = u192_is_zero(h), o = u192_is_ones(h, nbits);
   return fn_make(g - (z ? 1 : 0), g, g + (o ? 1 : 0));
 }
 
 // Add a delta in {-1,0,1} modulo 2^nbits.
-__device__ __forceinline__ void u192_add_delta(U192 &h, int d, int nbits) {
+__host__ __device__ __forceinline__ void u192_add_delta(U192 &h, int d, int nbits) {
   if (d != 0) (void)u192_add_s64(h, (long long)d, nbits);
 }
 

@@ -187,7 +187,7 @@ size_t ndigits(size_t XL, int b) { return (32 * (uint64_t)XL + b - 1) / b; }
 // 3-level shape adds a read+write of every operand and of the product.
 double shape_cost(const Shape &s) { return (double)s.M * (s.levels == 3 ? 2.0 : 1.0); }
 
-bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl) {
+bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl, size_t maxM = 0) {
   pl = Plan();
   pl.AL = std::min(AL, CL);
   pl.BL = std::min(BL, CL);
@@ -196,6 +196,7 @@ bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl)
   double best = 0;
   size_t first_fit = 0;
   for (size_t M : lengths()) {
+    if (maxM && M > maxM) break;
     if (g.forced_M && M != g.forced_M) continue;
     if (first_fit && M > 4 * first_fit) break;
     int bmax = std::min(width_limit(M), bcap);
@@ -248,62 +249,83 @@ double2 cis_neg(long double num, long double den, long double scale) {
   return make_double2((double)(cosl(a) * scale), (double)(-sinl(a) * scale));
 }
 
+// Offsets (in double2 entries) of each table inside one contiguous block.
+struct TableLayout {
+  size_t oL1 = 0, oL2 = 0, oLr = 0, opf = 0, opi = 0, olo = 0, ohi = 0, total = 0, nlo = 0;
+  int h = 0;
+  bool has_L2 = false, has_Lr = false, has_tw = false;
+};
+
+TableLayout table_layout(const Shape &s) {
+  TableLayout t;
+  const size_t four = 4 * (size_t)s.M;
+  while ((size_t(1) << (2 * t.h)) < four) t.h++;
+  t.nlo = size_t(1) << t.h;
+  const size_t nhi = (four + t.nlo - 1) / t.nlo;
+  t.has_L2 = s.levels == 3;
+  t.has_Lr = s.levels >= 2;
+  t.has_tw = s.levels >= 2;
+  size_t o = 0;
+  t.oL1 = o; o += s.L1;
+  if (t.has_L2) { t.oL2 = o; o += s.L2; }
+  if (t.has_Lr) { t.oLr = o; o += s.Lr; }
+  t.opf = o; o += s.L1;
+  t.opi = o; o += s.L1;
+  if (t.has_tw) { t.olo = o; o += t.nlo; t.ohi = o; o += nhi; }
+  t.total = o;
+  return t;
+}
+
+// All tables of a shape, computed in long double on the host into `host`
+// (t.total entries).
+void fill_tables(const Shape &s, const TableLayout &t, double2 *host) {
+  const size_t M = s.M, four = 4 * M;
+  auto block = [&](size_t at, size_t L) {
+    for (size_t m = 0; m < L; m++) host[at + m] = cis_neg((long double)m, (long double)L, 1.0L);
+  };
+  block(t.oL1, s.L1);
+  if (t.has_L2) block(t.oL2, s.L2);
+  if (t.has_Lr) block(t.oLr, s.Lr);
+  for (size_t n = 0; n < (size_t)s.L1; n++) {
+    // e^{+i pi n/(2 L1)} = conj(e^{-2 pi i n/(4 L1)}), and its conjugate / M
+    double2 w = cis_neg((long double)n, 4.0L * s.L1, 1.0L);
+    host[t.opf + n] = make_double2(w.x, -w.y);
+    host[t.opi + n] = cis_neg((long double)n, 4.0L * s.L1, 1.0L / (long double)M);
+  }
+  if (t.has_tw) {
+    const size_t nhi = t.ohi ? (four + t.nlo - 1) / t.nlo : 0;
+    for (size_t m = 0; m < t.nlo; m++) host[t.olo + m] = cis_neg((long double)m, (long double)four, 1.0L);
+    for (size_t m = 0; m < nhi; m++) host[t.ohi + m] = cis_neg((long double)(m * t.nlo), (long double)four, 1.0L);
+  }
+}
+
+Tables tables_at(const TableLayout &t, double2 *dev) {
+  Tables r;
+  r.dev = dev;
+  r.twL1 = dev + t.oL1;
+  r.twL2 = t.has_L2 ? dev + t.oL2 : nullptr;
+  r.twLr = t.has_Lr ? dev + t.oLr : nullptr;
+  r.pw_fwd = dev + t.opf;
+  r.pw_inv = dev + t.opi;
+  if (t.has_tw) {
+    r.tw4M.lo = dev + t.olo;
+    r.tw4M.hi = dev + t.ohi;
+    r.tw4M.mask = t.nlo - 1;
+    r.tw4M.h = t.h;
+  }
+  return r;
+}
+
 int ensure_tables(const Shape &s, Tables **out) {
   auto it = g.tables.find((size_t)s.M);
   if (it != g.tables.end()) { *out = &it->second; return BC_OK; }
-  const size_t M = s.M;
-  const size_t four = 4 * M;
-  int h = 0;
-  while ((size_t(1) << (2 * h)) < four) h++;
-  const size_t nlo = size_t(1) << h, nhi = (four + nlo - 1) / nlo;
-  const bool small = s.levels == 1;
-  const size_t nL2 = s.levels == 3 ? s.L2 : 0, nLr = s.levels >= 2 ? s.Lr : 0;
-  const size_t total = s.L1 + nL2 + nLr + 2 * (size_t)s.L1 + (small ? 0 : nlo + nhi);
-  std::vector<double2> host(total);
-  size_t o = 0;
-  auto block = [&](size_t L) {
-    for (size_t m = 0; m < L; m++) host[o + m] = cis_neg((long double)m, (long double)L, 1.0L);
-    size_t at = o;
-    o += L;
-    return at;
-  };
-  const size_t oL1 = block(s.L1);
-  const size_t oL2 = nL2 ? block(nL2) : 0;
-  const size_t oLr = nLr ? block(nLr) : 0;
-  const size_t opf = o;
-  for (size_t n = 0; n < (size_t)s.L1; n++) {
-    // e^{+i pi n/(2 L1)} = conj(e^{-2 pi i n/(4 L1)})
-    double2 w = cis_neg((long double)n, 4.0L * s.L1, 1.0L);
-    host[o + n] = make_double2(w.x, -w.y);
-  }
-  o += s.L1;
-  const size_t opi = o;
-  for (size_t n = 0; n < (size_t)s.L1; n++) host[o + n] = cis_neg((long double)n, 4.0L * s.L1, 1.0L / (long double)M);
-  o += s.L1;
-  size_t olo = 0, ohi = 0;
-  if (!small) {
-    olo = o;
-    for (size_t m = 0; m < nlo; m++) host[o + m] = cis_neg((long double)m, (long double)four, 1.0L);
-    o += nlo;
-    ohi = o;
-    for (size_t m = 0; m < nhi; m++) host[o + m] = cis_neg((long double)(m * nlo), (long double)four, 1.0L);
-    o += nhi;
-  }
-  Tables t;
-  CK(cudaMalloc(&t.dev, total * sizeof(double2)));
-  CK(cudaMemcpy(t.dev, host.data(), total * sizeof(double2), cudaMemcpyHostToDevice));
-  t.twL1 = t.dev + oL1;
-  t.twL2 = nL2 ? t.dev + oL2 : nullptr;
-  t.twLr = nLr ? t.dev + oLr : nullptr;
-  t.pw_fwd = t.dev + opf;
-  t.pw_inv = t.dev + opi;
-  if (!small) {
-    t.tw4M.lo = t.dev + olo;
-    t.tw4M.hi = t.dev + ohi;
-    t.tw4M.mask = nlo - 1;
-    t.tw4M.h = h;
-  }
-  auto res = g.tables.emplace(M, t);
+  const TableLayout lay = table_layout(s);
+  std::vector<double2> host(lay.total);
+  fill_tables(s, lay, host.data());
+  double2 *dev = nullptr;
+  CK(cudaMalloc(&dev, lay.total * sizeof(double2)));
+  CK(cudaMemcpy(dev, host.data(), lay.total * sizeof(double2), cudaMemcpyHostToDevice));
+  auto res = g.tables.emplace((size_t)s.M, tables_at(lay, dev));
   *out = &res.first->second;
   return BC_OK;
 }
@@ -398,22 +420,60 @@ int prepare(const KInfo &k, int *grid_cap) {
   return BC_OK;
 }
 
-int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunch) {
+int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunch, cudaStream_t stream,
+           bool timed) {
   int cap = 0;
   int r = prepare(k, &cap);
   if (r) return r;
   const int grid = (int)std::max<long long>(1, std::min<long long>(units, cap));
-  k.fn<<<grid, k.threads, k.smem, g.stream>>>(p);
+  k.fn<<<grid, k.threads, k.smem, stream>>>(p);
   CK(cudaGetLastError());
   (*nlaunch)++;
-  if (g.time_kernels) {
+  if (timed && g.time_kernels) {
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
-    CK(cudaEventRecord(e, g.stream));
+    CK(cudaEventRecord(e, stream));
     g.kev.push_back(e);
     g.ktimes.push_back({k.name, 0.0});
   }
   return BC_OK;
+}
+
+// The pass sequence of one class (all items share shape and squaring).
+// Scratch (buffers, records, lookback status, counter) must be set up and
+// the counter and status words zeroed by the caller.
+int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, unsigned long long carry_tiles,
+                 cudaStream_t stream, bool timed, size_t *nl) {
+  int r;
+  if (s.levels == 1) return launch(get_small(s.M, sq), n, p, nl, stream, timed);
+  const long long S1 = p.S1;
+  KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
+  const int W1 = ko.threads / (s.L1 / PTS);
+  if ((r = launch(ko, n * 2 * (S1 / W1), p, nl, stream, timed))) return r;
+  if (s.levels == 3) {
+    KInfo km = get_mid(s.L2, false);
+    const int W2 = km.threads / (s.L2 / PTS);
+    if ((r = launch(km, n * 2 * s.L1 * (s.Lr / W2), p, nl, stream, timed))) return r;
+  }
+  KInfo kr = get_rows(s.Lr, sq);
+  const int NR = kr.threads / (s.Lr / PTS);
+  if ((r = launch(kr, n * (s.M / s.Lr / NR), p, nl, stream, timed))) return r;
+  if (s.levels == 3) {
+    KInfo km = get_mid(s.L2, true);
+    const int W2 = km.threads / (s.L2 / PTS);
+    if ((r = launch(km, n * s.L1 * (s.Lr / W2), p, nl, stream, timed))) return r;
+  }
+  if ((r = launch(ki, n * (S1 / W1), p, nl, stream, timed))) return r;
+  KInfo kc{k_carry, CARRY_NT, 0, "carry"};
+  return launch(kc, (long long)carry_tiles, p, nl, stream, timed);
+}
+
+ClassParams class_params(const Shape &s, const Tables &tb) {
+  ClassParams p{};
+  p.M = s.M; p.L1 = s.L1; p.S1 = s.M / s.L1; p.L2 = s.L2; p.Lr = s.levels == 3 ? s.Lr : p.S1;
+  p.tw4M = tb.tw4M; p.pw_fwd = tb.pw_fwd; p.pw_inv = tb.pw_inv;
+  p.twL1 = tb.twL1; p.twL2 = tb.twL2; p.twLr = tb.twLr;
+  return p;
 }
 
 // ------------------------------------------------------------------ arena
@@ -591,42 +651,15 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     Tables *tb = nullptr;
     r = ensure_tables(s, &tb);
     if (r) return r;
-    ClassParams p{};
-    p.M = s.M; p.L1 = s.L1; p.S1 = s.M / s.L1; p.L2 = s.L2; p.Lr = s.levels == 3 ? s.Lr : p.S1;
-    p.tw4M = tb->tw4M; p.pw_fwd = tb->pw_fwd; p.pw_inv = tb->pw_inv;
-    p.twL1 = tb->twL1; p.twL2 = tb->twL2; p.twLr = tb->twLr;
+    ClassParams p = class_params(s, *tb);
     p.items = ddesc + first;
     p.nitems = (int)n;
     p.counter = ctr + 64 * cls;
     unsigned long long tiles = 0;
     for (size_t k = first; k < first + n; k++) tiles += works[order[k]]->pl.ntiles;
     p.carry_tiles = tiles;
-    size_t &nl = st->launches;
-    if (s.levels == 1) {
-      r = launch(get_small(s.M, sq), (long long)n, p, &nl);
-      if (r) return r;
-    } else {
-      const long long S1 = p.S1;
-      KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
-      const int W1 = ko.threads / (s.L1 / PTS);
-      if ((r = launch(ko, (long long)n * 2 * (S1 / W1), p, &nl))) return r;
-      if (s.levels == 3) {
-        KInfo km = get_mid(s.L2, false);
-        const int W2 = km.threads / (s.L2 / PTS);
-        if ((r = launch(km, (long long)n * 2 * s.L1 * (s.Lr / W2), p, &nl))) return r;
-      }
-      KInfo kr = get_rows(s.Lr, sq);
-      const int NR = kr.threads / (s.Lr / PTS);
-      if ((r = launch(kr, (long long)n * (s.M / s.Lr / NR), p, &nl))) return r;
-      if (s.levels == 3) {
-        KInfo km = get_mid(s.L2, true);
-        const int W2 = km.threads / (s.L2 / PTS);
-        if ((r = launch(km, (long long)n * s.L1 * (s.Lr / W2), p, &nl))) return r;
-      }
-      if ((r = launch(ki, (long long)n * (S1 / W1), p, &nl))) return r;
-      KInfo kc{k_carry, CARRY_NT, 0, "carry"};
-      if ((r = launch(kc, (long long)tiles, p, &nl))) return r;
-    }
+    (void)sq;
+    if ((r = launch_class(s, sq, p, (long long)n, tiles, g.stream, true, &st->launches))) return r;
     first += n;
     cls++;
   }

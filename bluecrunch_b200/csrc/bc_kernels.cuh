@@ -213,13 +213,13 @@ __global__ void __launch_bounds__((L / PTS) * NR, 1) k_rows(ClassParams p) {
 // ------------------------------------------------------------------ runs
 // 8 consecutive rounded coefficients c_u (exact integers held in doubles) ->
 // H = sum (bits of the running carry) and C = final signed carry.
-__device__ __forceinline__ void u192_or_bits(U192 &h, unsigned long long bits, int off) {
+__host__ __device__ __forceinline__ void u192_or_bits(U192 &h, unsigned long long bits, int off) {
   const int wi = off >> 6, bi = off & 63;
   h.w[wi] |= bits << bi;
   if (bi && wi < 2) h.w[wi + 1] |= bits >> (64 - bi);
 }
 
-__device__ __forceinline__ RunRec make_run(const double *c, int b) {
+__host__ __device__ __forceinline__ RunRec make_run(const double *c, int b) {
   U192 h = {{0, 0, 0}};
   long long acc = 0;
   const unsigned long long mask = (1ull << b) - 1;

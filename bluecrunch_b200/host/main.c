@@ -26,5 +26,11 @@ int main(int argc, char *argv[]) {
   task_start(0, "Starting calculation");
   int rc = bluecrunch_e(digits, mode, NULL);
   task_end(0);
+  if (getenv("BC_STATS")) {
+    bigfloat_mul_counters c;
+    bigfloat_get_counters(&c);
+    printf("GPU products: %zu in %zu calls, %.3f s inside GPU calls; host small products: %zu\n",
+           c.gpu_products, c.gpu_calls, c.gpu_seconds, c.small_products);
+  }
   return rc ? 1 : 0;
 }

@@ -81,6 +81,37 @@ static void ensure_gpu(void) {
   }
 }
 
+/* Optional FP64-free check of every GPU product (BC_VERIFY=1): A*B mod p for
+ * the reference's CHECKPRIME 0x9f063b05 and a second 32-bit prime, as the
+ * reference's DEBUG build checks every FFT product (bigfloat/mul.c:650-658).
+ * Only meaningful when CL >= AL+BL, which bigfloat_mul always passes. */
+static uint32_t residue(const uint32_t *T, size_t L, uint64_t p) {
+  uint64_t r = 0;
+  const uint64_t base = ((uint64_t)1 << 32) % p;
+  for (size_t i = L; i-- > 0;) r = ((r * base) % p + T[i] % p) % p;
+  return (uint32_t)r;
+}
+
+static int verify_on(void) {
+  static int v = -1;
+  if (v < 0) v = getenv("BC_VERIFY") != NULL;
+  return v;
+}
+
+static void verify(const uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B, size_t BL) {
+  static const uint64_t primes[2] = {0x9f063b05u, 4294967291u};
+  if (CL < AL + BL) return;
+  for (int k = 0; k < 2; k++) {
+    uint64_t p = primes[k];
+    uint64_t want = ((uint64_t)residue(A, AL, p) * residue(B, BL, p)) % p;
+    if (want != residue(C, CL, p)) {
+      fprintf(stderr, "bluecrunch: GPU product fails the modular check (AL=%zu BL=%zu CL=%zu prime %llx)\n",
+              AL, BL, CL, (unsigned long long)p);
+      abort();
+    }
+  }
+}
+
 static void count(size_t products, size_t calls, double secs) {
   pthread_mutex_lock(&g_cnt_mu);
   g_cnt.gpu_products += products;
@@ -99,6 +130,7 @@ int _fft_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *BT, siz
     fprintf(stderr, "_fft_mul: GPU multiply failed (CL=%zu): %s\n", CL, bc_gpu_strerror(rc));
     abort();
   }
+  if (verify_on() && CT != AT && CT != BT) verify(CT, CL, AT, AL, BT, BL);
   return st.width;
 }
 
@@ -119,6 +151,8 @@ void bc_host_gpu_batch(bc_gpu_item *items, size_t n) {
     fprintf(stderr, "bigfloat_mul_batch: GPU batch of %zu products failed: %s\n", n, bc_gpu_strerror(rc));
     abort();
   }
+  if (verify_on())
+    for (size_t i = 0; i < n; i++) verify(items[i].C, items[i].CL, items[i].A, items[i].AL, items[i].B, items[i].BL);
 }
 
 /* Exact schoolbook product of the low CL limbs (the value the reference's
