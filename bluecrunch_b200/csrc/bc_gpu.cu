@@ -982,3 +982,125 @@ int bc_gpu_kernel_times(const char **names, double *ms, int cap) {
 }
 
 }  // extern "C"
+
+// ====================================================================== allocation-free entry point
+// bc_gpu_mul_noalloc: the same exact product for callers that cannot
+// allocate device memory themselves or let a library do it — code running
+// inside a captured CUDA stream region, a custom allocator or memory pool
+// that owns the whole device, or an embedding host whose policy forbids
+// cudaMalloc after start-up.  Its scratch (transform buffers, run records,
+// lookback status, descriptor, error slots, twiddle tables) is one
+// file-scope __device__ array; the caller passes device inputs and outputs.
+namespace {
+constexpr size_t kNoAllocBytes = size_t(8) << 20;          // 8 MiB of scratch per GPU
+constexpr size_t kNoAllocMaxPoints = size_t(1) << 17;       // transforms up to 2^17 points
+constexpr size_t kNoAllocMaxLimbs = 131072;                 // AL + BL limit (fits 2^17 points at b = 16)
+constexpr size_t kNoAllocTableBytes = size_t(256) << 10;
+constexpr size_t kNoAllocDescOff = kNoAllocTableBytes;      // ItemDesc
+constexpr size_t kNoAllocSlotsOff = kNoAllocDescOff + 256;  // err (8 B), flags (4 B), counter (4 B)
+constexpr size_t kNoAllocStatusOff = kNoAllocSlotsOff + 256;
+constexpr size_t kNoAllocStatusBytes = 4096;                // lookback tiles: (2M/8)/256 * 4 B
+constexpr size_t kNoAllocWorkOff = kNoAllocStatusOff + kNoAllocStatusBytes;
+static_assert(kNoAllocWorkOff + 2 * 16 * kNoAllocMaxPoints + kNoAllocMaxPoints / 4 * sizeof(RunRec) <= kNoAllocBytes,
+              "no-alloc scratch too small");
+static_assert(sizeof(ItemDesc) <= 256, "descriptor slot");
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocDevice {
+  unsigned char *base;  // device address of the scratch array on this device
+  size_t table_M;       // transform length whose tables are in the scratch
+  int ready;
+};
+NoAllocDevice g_noalloc[kNoAllocMaxDevices];
+double2 g_noalloc_tables[kNoAllocTableBytes / sizeof(double2)];  // host staging for table uploads
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+extern "C" int bc_gpu_mul_noalloc(uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B,
+                                  size_t BL, void *stream_ptr) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  if (CL == 0) return BC_OK;
+  if (!C || (AL && !A) || (BL && !B)) return fail(BC_ERR_INVALID);
+  if (overlaps(C, CL * 4, A, AL * 4) || overlaps(C, CL * 4, B, BL * 4)) return fail(BC_ERR_INVALID);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(BC_ERR_INVALID);
+  NoAllocDevice &nd = g_noalloc[dev];
+  if (!nd.ready) {
+    // Set-up, once per device, with that device current: the array's name is
+    // only a host-side stand-in, so fetch its device address.
+    void *ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    nd.base = (unsigned char *)ptr;
+    nd.table_M = 0;
+    nd.ready = 1;
+  }
+  if (AL == 0 || BL == 0) {
+    CK(cudaMemsetAsync(C, 0, CL * 4, stream));
+    CK(cudaStreamSynchronize(stream));
+    return BC_OK;
+  }
+  if (std::min(AL, CL) + std::min(BL, CL) > kNoAllocMaxLimbs) return fail(BC_ERR_TOO_LARGE);
+  const bool square = A == B && AL == BL;
+  int bcap = 24;
+  for (int attempt = 0; attempt < 12; attempt++) {
+    Plan pl;
+    if (!make_plan(AL, BL, CL, square, bcap, pl, kNoAllocMaxPoints))
+      return fail(attempt ? BC_ERR_PRECISION : BC_ERR_TOO_LARGE);
+    const Shape &s = pl.shape;
+    const TableLayout lay = table_layout(s);
+    if (lay.total * sizeof(double2) > kNoAllocTableBytes || pl.ntiles * 4 > kNoAllocStatusBytes)
+      return fail(BC_ERR_TOO_LARGE);
+    if (nd.table_M != (size_t)s.M) {
+      CK(cudaStreamSynchronize(stream));  // the staging array and the old tables are no longer in use
+      fill_tables(s, lay, g_noalloc_tables);
+      CK(cudaMemcpyAsync(nd.base, g_noalloc_tables, lay.total * sizeof(double2), cudaMemcpyHostToDevice, stream));
+      nd.table_M = s.M;
+    }
+    unsigned char *w = nd.base + kNoAllocWorkOff;
+    const size_t M = s.M;
+    ItemDesc it{};
+    it.A = A;
+    it.B = square ? A : B;
+    it.C = C;
+    it.AL = pl.AL; it.BL = pl.BL; it.CL = CL;
+    it.ndA = pl.ndA; it.ndB = square ? pl.ndA : pl.ndB;
+    it.bufA = (double2 *)w;
+    it.bufB = square ? nullptr : (double2 *)(w + 16 * M);
+    it.rec = s.levels > 1 ? (RunRec *)(w + 32 * M) : nullptr;
+    it.status = s.levels > 1 ? (uint32_t *)(nd.base + kNoAllocStatusOff) : nullptr;
+    it.nwords = pl.nwords;
+    it.nruns = pl.nruns;
+    it.tile0 = 0;
+    it.err = (unsigned long long *)(nd.base + kNoAllocSlotsOff);
+    it.flags = (unsigned int *)(nd.base + kNoAllocSlotsOff + 8);
+    it.b = pl.b;
+    it.square = square ? 1 : 0;
+    ItemDesc *ddesc = (ItemDesc *)(nd.base + kNoAllocDescOff);
+    unsigned int *ctr = (unsigned int *)(nd.base + kNoAllocSlotsOff + 12);
+    // every call reuses the array: clear what the kernels expect to start at zero
+    CK(cudaMemcpyAsync(ddesc, &it, sizeof it, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(nd.base + kNoAllocSlotsOff, 0, 256 + kNoAllocStatusBytes, stream));
+    ClassParams p = class_params(s, tables_at(lay, (double2 *)nd.base));
+    p.items = ddesc;
+    p.nitems = 1;
+    p.counter = ctr;
+    p.carry_tiles = pl.ntiles;
+    size_t nl = 0;
+    int r = launch_class(s, square, p, 1, pl.ntiles, stream, false, &nl);
+    if (r) return r;
+    unsigned long long errbits = 0;
+    unsigned int flags = 0;
+    CK(cudaMemcpyAsync(&errbits, it.err, 8, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(&flags, it.flags, 4, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (flags & FLAG_TIMEOUT) return fail(BC_ERR_TIMEOUT);
+    double e;
+    memcpy(&e, &errbits, 8);
+    if (e < g.max_err && !(flags & FLAG_TOPCARRY)) return BC_OK;
+    bcap = pl.b - 1;  // narrower digits, as bc_gpu_mul retries
+  }
+  return fail(BC_ERR_PRECISION);
+}

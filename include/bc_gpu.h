@@ -119,6 +119,30 @@ int bc_gpu_lengths(size_t *out, int cap);
 /* Force transform length and width (0, 0 = automatic); for the autotuner. */
 int bc_gpu_force_plan(size_t fft_points, int width);
 
+/* Allocation-free product, for callers that cannot allocate device memory
+ * or have a library do it (inside a captured stream region, under a pool or
+ * allocator that owns the device, in hosts that forbid cudaMalloc after
+ * start-up).  No counterpart in the reference.
+ *
+ * C, A, B are device pointers of the current device; C must not overlap A or
+ * B.  Computes C[0..CL) = A*B mod 2^(32 CL) like bc_gpu_mul, on `stream`
+ * (cudaStream_t as void*, NULL = legacy default stream), and returns when the
+ * product is complete.  Limits: min(AL,CL) + min(BL,CL) <= 131072 limbs
+ * (transforms up to 2^17 points); larger products return BC_ERR_TOO_LARGE.
+ *
+ * Scratch is one 8 MiB file-scope __device__ array that every GPU loading
+ * this library holds until the process exits; nothing is allocated per call
+ * (no cudaMalloc/cudaFree or allocating library routine).  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Every call on a device shares
+ * the array and clears what must start at zero; calls whose GPU work
+ * overlaps would race on it.  The function serialises host callers and
+ * returns only after its work is complete, so overlap can only come from
+ * work enqueued around it (for example replaying a captured graph that
+ * contains it on two streams at once). */
+int bc_gpu_mul_noalloc(uint32_t *C, size_t CL, const uint32_t *A, size_t AL,
+                       const uint32_t *B, size_t BL, void *stream);
+
 int bc_gpu_sync(void);
 int bc_gpu_last_error(void);
 int bc_gpu_last_cuda_error(void);
