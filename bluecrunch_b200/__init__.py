@@ -82,6 +82,7 @@ GPU_SYMBOLS = {
     "bc_gpu_force_width": (ctypes.c_int, [ctypes.c_int]),
     "bc_gpu_force_plan": (ctypes.c_int, [_sz, ctypes.c_int]),
     "bc_gpu_lengths": (ctypes.c_int, [ctypes.POINTER(_sz), ctypes.c_int]),
+    "bc_gpu_check_shapes": (ctypes.c_int, []),
     "bc_gpu_load_width_table": (ctypes.c_int, [ctypes.c_char_p]),
     "bc_gpu_mul_noalloc": (ctypes.c_int, [ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz,
                                           ctypes.c_void_p]),

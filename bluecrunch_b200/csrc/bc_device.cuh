@@ -97,11 +97,12 @@ __device__ __forceinline__ void dftR(double2 *x) {
 // (natural order), so the first stage reads straight from global memory and
 // the last stage writes straight back, both coalesced across s.
 //
-// Shared-memory layout of a tile: W >= 8 columns: element (row, s) at
-// row*W + (s ^ ((s/8 + row) & 7)); the XOR keeps any 8 lanes that touch 8
-// consecutive columns of one row, or the same column of 8 consecutive rows,
-// or element e of 8 consecutive 8-column groups, on distinct bank groups.
-// W == 1 (one row per array): row + row/8 (one 16-byte pad per 8 elements).
+// Shared-memory layout of a tile (the layout a TMA load with 128-byte
+// swizzle writes): W >= 8 columns are W/8 boxes of L rows x 8 columns; the
+// 16-byte chunk of column c in row r of a box sits at chunk c ^ (r & 7).
+// A single row of L points (W == 1) is one box of L/8 lines of 8.  Any 8
+// lanes touching 8 columns of one row, one column of 8 consecutive rows, or
+// the Stockham scatter pattern land on distinct banks.
 
 constexpr int PTS = 8;
 
@@ -118,8 +119,8 @@ template <int L> struct Radices {
 template <int L, int W>
 __device__ __forceinline__ int sidx(int row, int s) {
   static_assert(W == 1 || W % 8 == 0, "tile width must be 1 or a multiple of 8");
-  if constexpr (W == 1) return row + (row >> 3);
-  else return row * W + (s ^ (((s >> 3) + row) & 7));
+  if constexpr (W == 1) return (row & ~7) + ((row & 7) ^ ((row >> 3) & 7));
+  else return (s >> 3) * (L * 8) + row * 8 + ((s & 7) ^ (row & 7));
 }
 
 template <int L, int W> struct TileSmem {
@@ -142,8 +143,17 @@ __device__ __forceinline__ void reg_stage(double2 (&v)[PTS], int t, const double
     if constexpr (NS > 1) {
       const int k = j % NS;
       constexpr int step = L / (NS * R);
+      if constexpr (R == 8) {
+        // w^1, w^2, w^4 from the table, the other powers by one product each
+        const double2 w1 = __ldg(&tw[k * step]), w2 = __ldg(&tw[2 * k * step]), w4 = __ldg(&tw[4 * k * step]);
+        const double2 w3 = cmul(w1, w2), w5 = cmul(w1, w4), w6 = cmul(w2, w4), w7 = cmul(w3, w4);
+        x[1] = ctw<INV>(x[1], w1); x[2] = ctw<INV>(x[2], w2); x[3] = ctw<INV>(x[3], w3);
+        x[4] = ctw<INV>(x[4], w4); x[5] = ctw<INV>(x[5], w5); x[6] = ctw<INV>(x[6], w6);
+        x[7] = ctw<INV>(x[7], w7);
+      } else {
 #pragma unroll
-      for (int r = 1; r < R; r++) x[r] = ctw<INV>(x[r], __ldg(&tw[k * r * step]));
+        for (int r = 1; r < R; r++) x[r] = ctw<INV>(x[r], __ldg(&tw[k * r * step]));
+      }
     }
     dftR<R, INV>(x);
 #pragma unroll

@@ -19,8 +19,10 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "bc_gpu.h"
-#include "bc_kernels.cuh"
+#include "bc_pipe.cuh"
 
 using namespace bc;
 
@@ -54,7 +56,7 @@ bool shape_for(size_t M, Shape &s) {
   for (int L1 : kOuterLens) {
     if (M % L1) continue;
     const size_t Lr = M / L1;
-    if (is_row_len(Lr) && pow2part(Lr) >= (size_t)(4096 / L1)) {
+    if (is_row_len(Lr) && pow2part(Lr) >= (size_t)std::max(8, 2048 / L1)) {
       s.M = (int)M; s.L1 = L1; s.L2 = 1; s.Lr = (int)Lr; s.levels = 2; return true;
     }
   }
@@ -66,7 +68,7 @@ bool shape_for(size_t M, Shape &s) {
       if (R % L1) continue;
       const size_t L2 = R / L1;
       if (L2 < 64 || L2 > 512 || (L2 & (L2 - 1)) || L2 > (size_t)L1) continue;
-      if (pow2part(Lr) < 4096 / L2) continue;
+      if (pow2part(Lr) < (size_t)std::max(8, 2048 / (int)L2) || pow2part(L2 * Lr) < (size_t)std::max(8, 2048 / L1)) continue;
       s.M = (int)M; s.L1 = L1; s.L2 = (int)L2; s.Lr = (int)Lr; s.levels = 3; return true;
     }
   }
@@ -331,49 +333,56 @@ int ensure_tables(const Shape &s, Tables **out) {
 }
 
 // ------------------------------------------------------------------ kernels
-typedef void (*KFn)(ClassParams);
-
-template <int L> constexpr int rows_per_cta() {
-  constexpr int tc = L / PTS;
-  return tc >= 256 ? 1 : (256 / tc >= 16 ? 16 : (256 / tc >= 8 ? 8 : (256 / tc >= 4 ? 4 : (256 / tc >= 2 ? 2 : 1))));
-}
+// Kernel parameter lists: (ClassParams), (ClassParams, map), (ClassParams, map, map).
+enum KSig { SIG_P = 0, SIG_P_MAP = 1, SIG_P_MAP2 = 2 };
 
 struct KInfo {
-  KFn fn = nullptr;
+  const void *fn = nullptr;
   int threads = 0;
   size_t smem = 0;
   const char *name = "";
+  int sig = SIG_P;
+  int box = 0;            // TMA box lines (rows) the kernel expects per box
+  unsigned unit_bytes = 0; // bytes the kernel waits for per staged unit (per operand)
+  int parts = 1;          // boxes per column group (or per row)
 };
 
-template <int L, int W>
+template <int L>
 KInfo outer_fwd_info() {
-  return {k_outer_fwd<L, W>, (L / PTS) * W, TileSmem<L, W>::elems * sizeof(double2), "outer_fwd"};
+  using T = PassTile<L>;
+  using K = PackTile<L>;
+  return {(const void *)k2_outer_fwd<L>, T::NT, (size_t)L * T::W * 16 + 2 * (size_t)K::STAGE_WORDS * 4 + 1024,
+          "outer_fwd", SIG_P};
 }
-template <int L, int W>
+template <int L>
 KInfo outer_inv_info() {
-  return {k_outer_inv<L, W>, (L / PTS) * W, TileSmem<L, W>::elems * sizeof(double2), "outer_inv"};
+  using T = PassTile<L>;
+  return {(const void *)k2_outer_inv<L>, T::NT, 2 * (size_t)L * T::W * 16 + 1024, "outer_inv", SIG_P_MAP,
+          T::BOX_ROWS, T::BYTES, T::HALVES};
 }
 template <int L, bool INV>
 KInfo mid_info() {
-  constexpr int W = 4096 / L;
-  return {k_mid<L, W, INV>, (L / PTS) * W, TileSmem<L, W>::elems * sizeof(double2), INV ? "mid_inv" : "mid_fwd"};
+  using T = PassTile<L>;
+  return {(const void *)k2_mid<L, INV>, T::NT, 2 * (size_t)L * T::W * 16 + 1024, INV ? "mid_inv" : "mid_fwd",
+          SIG_P_MAP2, T::BOX_ROWS, T::BYTES, T::HALVES};
 }
 template <int L, bool SQ>
 KInfo rows_info() {
-  constexpr int NR = rows_per_cta<L>();
-  return {k_rows<L, NR, SQ>, (L / PTS) * NR, (size_t)NR * TileSmem<L, 1>::elems * sizeof(double2), "rows"};
+  using R = RowTile<L>;
+  return {(const void *)k2_rows<L, SQ>, R::NT, 3 * (size_t)R::NR * L * 16 + 1024, "rows", SIG_P_MAP2,
+          R::BOX_LINES, (unsigned)(R::NR * L * 16), R::PARTS};
 }
 template <int M, bool SQ>
 KInfo small_info() {
-  return {k_small<M, SQ>, M / PTS, TileSmem<M, 1>::elems * sizeof(double2), "small"};
+  return {(const void *)k_small<M, SQ>, M / PTS, TileSmem<M, 1>::elems * sizeof(double2), "small", SIG_P};
 }
 
 KInfo get_outer(int L, bool inv) {
   switch (L) {
-    case 64: return inv ? outer_inv_info<64, 64>() : outer_fwd_info<64, 64>();
-    case 128: return inv ? outer_inv_info<128, 32>() : outer_fwd_info<128, 32>();
-    case 256: return inv ? outer_inv_info<256, 16>() : outer_fwd_info<256, 16>();
-    case 512: return inv ? outer_inv_info<512, 8>() : outer_fwd_info<512, 8>();
+    case 64: return inv ? outer_inv_info<64>() : outer_fwd_info<64>();
+    case 128: return inv ? outer_inv_info<128>() : outer_fwd_info<128>();
+    case 256: return inv ? outer_inv_info<256>() : outer_fwd_info<256>();
+    case 512: return inv ? outer_inv_info<512>() : outer_fwd_info<512>();
   }
   return {};
 }
@@ -405,14 +414,14 @@ KInfo get_small(int M, bool sq) {
   return {};
 }
 
-std::map<KFn, int> g_occ;  // resident CTAs per SM, per kernel
+std::map<const void *, int> g_occ;  // resident CTAs per SM, per kernel
 
 int prepare(const KInfo &k, int *grid_cap) {
   auto it = g_occ.find(k.fn);
   if (it == g_occ.end()) {
-    if (k.smem > 48 * 1024) CK(cudaFuncSetAttribute((const void *)k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+    if (k.smem > 48 * 1024) CK(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
     int n = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void *)k.fn, k.threads, k.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k.fn, k.threads, k.smem));
     if (n < 1) n = 1;
     it = g_occ.emplace(k.fn, n).first;
   }
@@ -420,14 +429,19 @@ int prepare(const KInfo &k, int *grid_cap) {
   return BC_OK;
 }
 
-int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunch, cudaStream_t stream,
-           bool timed) {
+int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunch, cudaStream_t stream, bool timed,
+           const CUtensorMap *mA = nullptr, const CUtensorMap *mB = nullptr) {
   int cap = 0;
   int r = prepare(k, &cap);
   if (r) return r;
   const int grid = (int)std::max<long long>(1, std::min<long long>(units, cap));
-  k.fn<<<grid, k.threads, k.smem, stream>>>(p);
-  CK(cudaGetLastError());
+  ClassParams pc = p;
+  CUtensorMap a{}, b{};
+  if (mA) a = *mA;
+  if (mB) b = *mB;
+  else b = a;
+  void *args[3] = {&pc, &a, &b};
+  CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
   (*nlaunch)++;
   if (timed && g.time_kernels) {
     cudaEvent_t e;
@@ -439,32 +453,123 @@ int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunc
   return BC_OK;
 }
 
-// The pass sequence of one class (all items share shape and squaring).
-// Scratch (buffers, records, lookback status, counter) must be set up and
-// the counter and status words zeroed by the caller.
-int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, unsigned long long carry_tiles,
-                 cudaStream_t stream, bool timed, size_t *nl) {
-  int r;
-  if (s.levels == 1) return launch(get_small(s.M, sq), n, p, nl, stream, timed);
-  const long long S1 = p.S1;
-  KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
+// ------------------------------------------------------------------ tensor maps
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int get_encoder() {
+  if (g_encode) return BC_OK;
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q));
+  if (q != cudaDriverEntryPointSuccess || !fn) return fail(BC_ERR_CUDA);
+  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  return BC_OK;
+}
+
+// FLOAT64 elements, 128-byte swizzle, innermost box dimension 16 doubles.
+int encode_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+               const cuuint32_t *box) {
+  int r = get_encoder();
+  if (r) return r;
+  cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  CUresult cr = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void *>(base), dims, strides,
+                         box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) {
+    if (g.verbose) fprintf(stderr, "bc_gpu: cuTensorMapEncodeTiled failed (%d)\n", (int)cr);
+    return fail(BC_ERR_CUDA);
+  }
+  return BC_OK;
+}
+
+// Host-side consistency of a shape's pipelined launches: every staged unit's
+// TMA boxes must deliver exactly the bytes its kernel waits for, boxes must
+// tile the rows, and column tiles must tile the rows of each pass.  Checked
+// before every launch and, for all lengths, by bc_gpu_check_shapes.
+bool shape_launch_ok(const Shape &s, bool sq) {
+  if (s.levels == 1) return get_small(s.M, sq).fn != nullptr;
+  const size_t S1 = s.M / s.L1, Lr = s.levels == 3 ? (size_t)s.Lr : S1;
+  KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true), kr = get_rows((int)Lr, sq);
+  if (!ko.fn || !ki.fn || !kr.fn) return false;
   const int W1 = ko.threads / (s.L1 / PTS);
-  if ((r = launch(ko, n * 2 * (S1 / W1), p, nl, stream, timed))) return r;
+  if (S1 % W1 || W1 % 8) return false;
+  if ((size_t)(W1 / 8) * ki.parts * 128 * ki.box != ki.unit_bytes || (size_t)ki.box * ki.parts != (size_t)s.L1)
+    return false;
+  const int NR = kr.threads / ((int)Lr / PTS);
+  if ((size_t)kr.parts * 128 * kr.box * NR != kr.unit_bytes || (size_t)kr.box * kr.parts != Lr / 8 ||
+      (s.M / Lr) % NR != 0 || kr.box > 256 || kr.box % 8)
+    return false;
   if (s.levels == 3) {
     KInfo km = get_mid(s.L2, false);
+    if (!km.fn) return false;
     const int W2 = km.threads / (s.L2 / PTS);
-    if ((r = launch(km, n * 2 * s.L1 * (s.Lr / W2), p, nl, stream, timed))) return r;
+    if (Lr % W2 || W2 % 8) return false;
+    if ((size_t)(W2 / 8) * km.parts * 128 * km.box != km.unit_bytes || (size_t)km.box * km.parts != (size_t)s.L2)
+      return false;
   }
-  KInfo kr = get_rows(s.Lr, sq);
-  const int NR = kr.threads / (s.Lr / PTS);
-  if ((r = launch(kr, n * (s.M / s.Lr / NR), p, nl, stream, timed))) return r;
+  return true;
+}
+
+// The pass sequence of one class (all items share shape and squaring).  The
+// items' A and B buffers are the contiguous slabs slabA / slabB (item i at
+// i*M).  Scratch (records, lookback status, counter) must be set up and the
+// counter and status words zeroed by the caller.
+int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, unsigned long long carry_tiles,
+                 double2 *slabA, double2 *slabB, cudaStream_t stream, bool timed, size_t *nl) {
+  int r;
+  if (!shape_launch_ok(s, sq)) return fail(BC_ERR_INVALID);
+  if (s.levels == 1) return launch(get_small(s.M, sq), n, p, nl, stream, timed);
+  const cuuint64_t M16 = (cuuint64_t)s.M * 16, S1 = (cuuint64_t)p.S1, Lr = (cuuint64_t)p.Lr;
+  KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
+  const int W1 = ko.threads / (s.L1 / PTS);
+  const int nops = sq ? 1 : 2;
+  if ((r = launch(ko, n * nops * (long long)(S1 / W1), p, nl, stream, timed))) return r;
+  CUtensorMap midA, midB;
+  if (s.levels == 3) {
+    const cuuint64_t dims[4] = {2 * Lr, (cuuint64_t)s.L2, (cuuint64_t)s.L1, (cuuint64_t)n};
+    const cuuint64_t str[3] = {Lr * 16, S1 * 16, M16};
+    KInfo km = get_mid(s.L2, false);
+    const int W2 = km.threads / (s.L2 / PTS);
+    const cuuint32_t box[4] = {16, (cuuint32_t)km.box, 1, 1};
+    // the boxes of one tile must deliver exactly what the kernel waits for
+    if ((size_t)(W2 / 8) * km.parts * 128 * km.box != km.unit_bytes || (size_t)km.box * km.parts != (size_t)s.L2)
+      return fail(BC_ERR_INVALID);
+    if ((r = encode_map(&midA, slabA, 4, dims, str, box))) return r;
+    if (!sq && (r = encode_map(&midB, slabB, 4, dims, str, box))) return r;
+    if ((r = launch(km, n * nops * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB)))
+      return r;
+  }
+  {
+    KInfo kr = get_rows(s.Lr, sq);
+    const int NR = kr.threads / (s.Lr / PTS);
+    const cuuint64_t rows = (cuuint64_t)n * (cuuint64_t)(s.M / s.Lr);
+    const cuuint64_t dims[3] = {16, Lr / 8, rows};
+    const cuuint64_t str[2] = {128, Lr * 16};
+    const cuuint32_t box[3] = {16, (cuuint32_t)kr.box, (cuuint32_t)NR};
+    if ((size_t)kr.parts * 128 * kr.box * NR != kr.unit_bytes || (size_t)kr.box * kr.parts != (size_t)(Lr / 8) ||
+        (s.M / s.Lr) % NR != 0)
+      return fail(BC_ERR_INVALID);
+    CUtensorMap rA, rB;
+    if ((r = encode_map(&rA, slabA, 3, dims, str, box))) return r;
+    if (!sq && (r = encode_map(&rB, slabB, 3, dims, str, box))) return r;
+    if ((r = launch(kr, (long long)(rows / NR), p, nl, stream, timed, &rA, sq ? &rA : &rB))) return r;
+  }
   if (s.levels == 3) {
     KInfo km = get_mid(s.L2, true);
     const int W2 = km.threads / (s.L2 / PTS);
-    if ((r = launch(km, n * s.L1 * (s.Lr / W2), p, nl, stream, timed))) return r;
+    if ((r = launch(km, n * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, &midA))) return r;
   }
-  if ((r = launch(ki, n * (S1 / W1), p, nl, stream, timed))) return r;
-  KInfo kc{k_carry, CARRY_NT, 0, "carry"};
+  {
+    const cuuint64_t dims[3] = {2 * S1, (cuuint64_t)s.L1, (cuuint64_t)n};
+    const cuuint64_t str[2] = {S1 * 16, M16};
+    const cuuint32_t box[3] = {16, (cuuint32_t)ki.box, 1};
+    if ((size_t)(W1 / 8) * ki.parts * 128 * ki.box != ki.unit_bytes || (size_t)ki.box * ki.parts != (size_t)s.L1)
+      return fail(BC_ERR_INVALID);
+    CUtensorMap oA;
+    if ((r = encode_map(&oA, slabA, 3, dims, str, box))) return r;
+    if ((r = launch(ki, n * (long long)(S1 / W1), p, nl, stream, timed, &oA))) return r;
+  }
+  KInfo kc{(const void *)k_carry, CARRY_NT, 0, "carry", SIG_P};
   return launch(kc, (long long)carry_tiles, p, nl, stream, timed);
 }
 
@@ -541,14 +646,43 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }
 
 // Run one attempt over `works` (all not done).  Fills err/flags.
+// Pinned host staging for small operands and results: one host-to-device
+// and one device-to-host copy per batch instead of one per item.
+constexpr size_t kStageItemMax = size_t(1) << 20;  // bytes; larger arrays copy directly
+
+struct PinnedStage {
+  char *p = nullptr;
+  size_t cap = 0;
+};
+PinnedStage g_pin_in, g_pin_out;
+
+int pinned_reserve(PinnedStage &ps, size_t bytes) {
+  if (bytes <= ps.cap) return BC_OK;
+  if (ps.p) CK(cudaFreeHost(ps.p));
+  ps.p = nullptr;
+  ps.cap = 0;
+  size_t want = std::max(bytes + bytes / 2, (size_t)1 << 22);
+  CK(cudaHostAlloc((void **)&ps.p, want, cudaHostAllocDefault));
+  ps.cap = want;
+  return BC_OK;
+}
+
+// Run one attempt over `works` (none done yet).  Fills err/flags and copies
+// out the products that pass the rounding check.
 int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st) {
+  const size_t nw = works.size();
+  // ---- classes (M, square); items of a class get contiguous slabs
+  std::map<std::pair<size_t, bool>, std::vector<size_t>> classes;
+  for (size_t i = 0; i < nw; i++) classes[{(size_t)works[i]->pl.shape.M, works[i]->pl.square}].push_back(i);
+
   // ---- memory layout
-  struct Slot { size_t off_dA, off_dB, off_dC, off_work, off_desc; };
-  std::vector<Slot> slots(works.size());
-  size_t off = 0;
-  std::vector<Run> runs(works.size());
-  std::vector<char> hostA(works.size()), hostB(works.size());
-  for (size_t i = 0; i < works.size(); i++) {
+  struct Slot { size_t off_dA = 0, off_dB = 0, off_dC = 0, off_rec = 0, off_status = 0; };
+  std::vector<Slot> slots(nw);
+  std::vector<Run> runs(nw);
+  std::vector<char> hostA(nw), hostB(nw);
+  size_t off = 0, stage_in = 0, stage_out = 0;
+  std::vector<size_t> pin_in_off(nw, SIZE_MAX), pin_inB_off(nw, SIZE_MAX), pin_out_off(nw, SIZE_MAX);
+  for (size_t i = 0; i < nw; i++) {
     const bc_mul_desc &d = items[works[i]->idx];
     const Plan &pl = works[i]->pl;
     hostA[i] = pl.AL && !is_device_ptr(d.A);
@@ -558,65 +692,101 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     slots[i].off_dA = off; if (hostA[i]) off += align256(pl.AL * 4);
     slots[i].off_dB = off; if (hostB[i]) off += align256(pl.BL * 4);
     slots[i].off_dC = off; if (runs[i].hostC || runs[i].stagedC) off += align256(d.CL * 4);
-    slots[i].off_work = off; off += work_bytes(pl);
+    if (hostA[i] && pl.AL * 4 <= kStageItemMax) { pin_in_off[i] = stage_in; stage_in += align256(pl.AL * 4); }
+    if (hostB[i] && pl.BL * 4 <= kStageItemMax) { pin_inB_off[i] = stage_in; stage_in += align256(pl.BL * 4); }
+    if (runs[i].hostC && d.CL * 4 <= kStageItemMax) { pin_out_off[i] = stage_out; stage_out += align256(d.CL * 4); }
   }
-  const size_t off_err = off; off += align256(works.size() * 8);
-  const size_t off_flags = off; off += align256(works.size() * 4);
-  const size_t off_desc = off; off += align256(works.size() * sizeof(ItemDesc));
-  const size_t off_ctr = off; off += 256 * (works.size() + 1);
+  // the staged inputs sit contiguously in the arena so one copy moves them
+  const size_t off_stage_in = off;
+  off += align256(stage_in);
+  struct ClassSlab { size_t offA = 0, offB = 0; };
+  std::map<std::pair<size_t, bool>, ClassSlab> slab;
+  for (auto &c : classes) {
+    const size_t M = c.first.first, n = c.second.size();
+    ClassSlab cs;
+    cs.offA = off; off += n * align256(M * 16);
+    if (!c.first.second) { cs.offB = off; off += n * align256(M * 16); }
+    slab[c.first] = cs;
+  }
+  size_t status_words = 0;
+  for (size_t i = 0; i < nw; i++) {
+    const Plan &pl = works[i]->pl;
+    if (pl.shape.levels > 1) {
+      slots[i].off_rec = off;
+      off += align256((size_t)pl.shape.M / 4 * sizeof(RunRec));
+      slots[i].off_status = status_words;
+      status_words += pl.ntiles;
+    }
+  }
+  // err, flags, counters and status words: one region, cleared by one memset
+  const size_t off_err = off; off += align256(nw * 8);
+  const size_t off_flags = off; off += align256(nw * 4);
+  const size_t off_ctr = off; off += 256 * (classes.size() + 1);
+  const size_t off_status = off; off += align256(status_words * 4);
+  const size_t zero_end = off;
+  const size_t off_desc = off; off += align256(nw * sizeof(ItemDesc));
   int r = arena_reserve(off);
   if (r) return r;
   char *base = g.arena;
 
-  auto t_h2d = std::chrono::steady_clock::now();
   // ---- inputs
-  for (size_t i = 0; i < works.size(); i++) {
+  if (stage_in) {
+    if ((r = pinned_reserve(g_pin_in, stage_in))) return r;
+    for (size_t i = 0; i < nw; i++) {
+      const bc_mul_desc &d = items[works[i]->idx];
+      if (pin_in_off[i] != SIZE_MAX) memcpy(g_pin_in.p + pin_in_off[i], d.A, works[i]->pl.AL * 4);
+      if (pin_inB_off[i] != SIZE_MAX) memcpy(g_pin_in.p + pin_inB_off[i], d.B, works[i]->pl.BL * 4);
+    }
+    CK(cudaMemcpyAsync(base + off_stage_in, g_pin_in.p, stage_in, cudaMemcpyHostToDevice, g.stream));
+    st->h2d_bytes += stage_in;
+  }
+  for (size_t i = 0; i < nw; i++) {
     const bc_mul_desc &d = items[works[i]->idx];
     const Plan &pl = works[i]->pl;
-    runs[i].dA = hostA[i] ? (const uint32_t *)(base + slots[i].off_dA) : d.A;
-    if (hostA[i]) {
+    if (!hostA[i]) runs[i].dA = d.A;
+    else if (pin_in_off[i] != SIZE_MAX) runs[i].dA = (const uint32_t *)(base + off_stage_in + pin_in_off[i]);
+    else {
+      runs[i].dA = (const uint32_t *)(base + slots[i].off_dA);
       CK(cudaMemcpyAsync((void *)runs[i].dA, d.A, pl.AL * 4, cudaMemcpyHostToDevice, g.stream));
       st->h2d_bytes += pl.AL * 4;
     }
     if (pl.square) runs[i].dB = runs[i].dA;
+    else if (!hostB[i]) runs[i].dB = d.B;
+    else if (pin_inB_off[i] != SIZE_MAX) runs[i].dB = (const uint32_t *)(base + off_stage_in + pin_inB_off[i]);
     else {
-      runs[i].dB = hostB[i] ? (const uint32_t *)(base + slots[i].off_dB) : d.B;
-      if (hostB[i]) {
-        CK(cudaMemcpyAsync((void *)runs[i].dB, d.B, pl.BL * 4, cudaMemcpyHostToDevice, g.stream));
-        st->h2d_bytes += pl.BL * 4;
-      }
+      runs[i].dB = (const uint32_t *)(base + slots[i].off_dB);
+      CK(cudaMemcpyAsync((void *)runs[i].dB, d.B, pl.BL * 4, cudaMemcpyHostToDevice, g.stream));
+      st->h2d_bytes += pl.BL * 4;
     }
     runs[i].dC = (runs[i].hostC || runs[i].stagedC) ? (uint32_t *)(base + slots[i].off_dC) : d.C;
   }
-  CK(cudaMemsetAsync(base + off_err, 0, off_desc - off_err, g.stream));
+  CK(cudaMemsetAsync(base + off_err, 0, zero_end - off_err, g.stream));
 
-  // ---- descriptors, grouped by class (M, square)
-  std::map<std::pair<size_t, bool>, std::vector<size_t>> classes;
-  for (size_t i = 0; i < works.size(); i++) classes[{(size_t)works[i]->pl.shape.M, works[i]->pl.square}].push_back(i);
-  std::vector<ItemDesc> desc(works.size());
+  // ---- descriptors
+  std::vector<ItemDesc> desc(nw);
   std::vector<size_t> order;
-  order.reserve(works.size());
+  order.reserve(nw);
   for (auto &c : classes) {
     unsigned long long tile0 = 0;
+    const ClassSlab &cs = slab[c.first];
+    size_t k = 0;
     for (size_t i : c.second) {
       const bc_mul_desc &d = items[works[i]->idx];
       const Plan &pl = works[i]->pl;
       ItemDesc &it = desc[order.size()];
       order.push_back(i);
-      char *w = base + slots[i].off_work;
       const size_t M = pl.shape.M;
       it.A = runs[i].dA;
       it.B = runs[i].dB;
       it.C = runs[i].dC;
       it.AL = pl.AL; it.BL = pl.BL; it.CL = d.CL;
       it.ndA = pl.ndA; it.ndB = pl.square ? pl.ndA : pl.ndB;
-      it.bufA = (double2 *)w; w += align256(M * 16);
-      it.bufB = nullptr;
-      if (!pl.square) { it.bufB = (double2 *)w; w += align256(M * 16); }
+      it.bufA = (double2 *)(base + cs.offA + k * align256(M * 16));
+      it.bufB = pl.square ? nullptr : (double2 *)(base + cs.offB + k * align256(M * 16));
       it.rec = nullptr; it.status = nullptr;
       if (pl.shape.levels > 1) {
-        it.rec = (RunRec *)w; w += align256(M / 4 * sizeof(RunRec));
-        it.status = (uint32_t *)w; w += align256(pl.ntiles * 4);
+        it.rec = (RunRec *)(base + slots[i].off_rec);
+        it.status = (uint32_t *)(base + off_status) + slots[i].off_status;
       }
       it.nwords = pl.nwords;
       it.nruns = pl.nruns;
@@ -626,19 +796,12 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
       it.flags = (unsigned int *)(base + off_flags) + i;
       it.b = pl.b;
       it.square = pl.square ? 1 : 0;
+      k++;
     }
   }
-  // status words must start at zero for every attempt
-  for (size_t k = 0; k < order.size(); k++) {
-    const ItemDesc &it = desc[k];
-    if (it.status) CK(cudaMemsetAsync(it.status, 0, works[order[k]]->pl.ntiles * 4, g.stream));
-  }
   ItemDesc *ddesc = (ItemDesc *)(base + off_desc);
-  CK(cudaMemcpyAsync(ddesc, desc.data(), desc.size() * sizeof(ItemDesc), cudaMemcpyHostToDevice, g.stream));
+  CK(cudaMemcpyAsync(ddesc, desc.data(), nw * sizeof(ItemDesc), cudaMemcpyHostToDevice, g.stream));
   unsigned int *ctr = (unsigned int *)(base + off_ctr);
-  CK(cudaMemsetAsync(ctr, 0, 256 * (works.size() + 1), g.stream));
-  const double h2d_ms = ms_since(t_h2d);
-  (void)h2d_ms;
 
   // ---- launches
   CK(cudaEventRecord(g.ev0, g.stream));
@@ -654,12 +817,15 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     ClassParams p = class_params(s, *tb);
     p.items = ddesc + first;
     p.nitems = (int)n;
+    p.sq = sq ? 1 : 0;
     p.counter = ctr + 64 * cls;
     unsigned long long tiles = 0;
     for (size_t k = first; k < first + n; k++) tiles += works[order[k]]->pl.ntiles;
     p.carry_tiles = tiles;
-    (void)sq;
-    if ((r = launch_class(s, sq, p, (long long)n, tiles, g.stream, true, &st->launches))) return r;
+    const ClassSlab &cs = slab[c.first];
+    if ((r = launch_class(s, sq, p, (long long)n, tiles, (double2 *)(base + cs.offA),
+                          sq ? nullptr : (double2 *)(base + cs.offB), g.stream, true, &st->launches)))
+      return r;
     first += n;
     cls++;
   }
@@ -667,10 +833,10 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   st->classes += classes.size();
 
   // ---- verdicts, then outputs of the products that passed
-  std::vector<unsigned long long> errs(works.size());
-  std::vector<unsigned> flags(works.size());
-  CK(cudaMemcpyAsync(errs.data(), base + off_err, works.size() * 8, cudaMemcpyDeviceToHost, g.stream));
-  CK(cudaMemcpyAsync(flags.data(), base + off_flags, works.size() * 4, cudaMemcpyDeviceToHost, g.stream));
+  std::vector<unsigned long long> errs(nw);
+  std::vector<unsigned> flags(nw);
+  CK(cudaMemcpyAsync(errs.data(), base + off_err, nw * 8, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaMemcpyAsync(flags.data(), base + off_flags, nw * 4, cudaMemcpyDeviceToHost, g.stream));
   CK(cudaStreamSynchronize(g.stream));
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, g.ev0, g.ev1));
@@ -686,17 +852,24 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     for (auto e : g.kev) cudaEventDestroy(e);
     g.kev.clear();
   }
-  bool copies = false;
-  for (size_t i = 0; i < works.size(); i++) {
+  if (stage_out && (r = pinned_reserve(g_pin_out, stage_out))) return r;
+  bool copies = false, staged_out = false;
+  std::vector<char> ok(nw);
+  for (size_t i = 0; i < nw; i++) {
     double e;
     memcpy(&e, &errs[i], 8);
     works[i]->err = e;
     works[i]->flags = flags[i];
-    const bool ok = ((e < g.max_err) && !(flags[i] & FLAG_TOPCARRY)) || g.forced_width;
+    ok[i] = (((e < g.max_err) && !(flags[i] & FLAG_TOPCARRY)) || g.forced_width) && !(flags[i] & FLAG_TIMEOUT);
     const bc_mul_desc &d = items[works[i]->idx];
-    if (!ok || flags[i] & FLAG_TIMEOUT) continue;
+    if (!ok[i]) continue;
     if (runs[i].hostC) {
-      CK(cudaMemcpyAsync(d.C, runs[i].dC, d.CL * 4, cudaMemcpyDeviceToHost, g.stream));
+      if (pin_out_off[i] != SIZE_MAX) {
+        CK(cudaMemcpyAsync(g_pin_out.p + pin_out_off[i], runs[i].dC, d.CL * 4, cudaMemcpyDeviceToHost, g.stream));
+        staged_out = true;
+      } else {
+        CK(cudaMemcpyAsync(d.C, runs[i].dC, d.CL * 4, cudaMemcpyDeviceToHost, g.stream));
+      }
       st->d2h_bytes += d.CL * 4;
       copies = true;
     } else if (runs[i].stagedC) {
@@ -705,6 +878,9 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     }
   }
   if (copies) CK(cudaStreamSynchronize(g.stream));
+  if (staged_out)
+    for (size_t i = 0; i < nw; i++)
+      if (ok[i] && pin_out_off[i] != SIZE_MAX) memcpy(items[works[i]->idx].C, g_pin_out.p + pin_out_off[i], items[works[i]->idx].CL * 4);
   return BC_OK;
 }
 
@@ -920,6 +1096,16 @@ int bc_gpu_load_width_table(const char *path) {
   return BC_OK;
 }
 
+int bc_gpu_check_shapes(void) {
+  for (size_t M : lengths()) {
+    Shape s;
+    if (!shape_for(M, s)) return (int)std::min<size_t>(M, 0x7fffffff);
+    for (int sq = 0; sq < 2; sq++)
+      if (!shape_launch_ok(s, sq != 0)) return (int)std::min<size_t>(M, 0x7fffffff);
+  }
+  return BC_OK;
+}
+
 int bc_gpu_lengths(size_t *out, int cap) {
   const std::vector<size_t> &v = lengths();
   for (int i = 0; i < cap && i < (int)v.size(); i++) out[i] = v[i];
@@ -1086,10 +1272,11 @@ extern "C" int bc_gpu_mul_noalloc(uint32_t *C, size_t CL, const uint32_t *A, siz
     ClassParams p = class_params(s, tables_at(lay, (double2 *)nd.base));
     p.items = ddesc;
     p.nitems = 1;
+    p.sq = square ? 1 : 0;
     p.counter = ctr;
     p.carry_tiles = pl.ntiles;
     size_t nl = 0;
-    int r = launch_class(s, square, p, 1, pl.ntiles, stream, false, &nl);
+    int r = launch_class(s, square, p, 1, pl.ntiles, it.bufA, it.bufB, stream, false, &nl);
     if (r) return r;
     unsigned long long errbits = 0;
     unsigned int flags = 0;

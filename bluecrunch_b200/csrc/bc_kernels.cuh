@@ -61,6 +61,7 @@ struct ClassParams {
   const double2 *twL1, *twL2, *twLr;  // e^{-2 pi i m/L}
   const ItemDesc *items;
   int nitems;
+  int sq;                 // every item of the class squares (one operand)
   unsigned int *counter;  // k_carry dynamic tile counter (zeroed before launch)
   unsigned long long carry_tiles;  // total k_carry tiles over the class
 };
@@ -252,7 +253,7 @@ __device__ __forceinline__ RunRec load_rec(const RunRec *src) {
 template <int L, int W>
 __global__ void __launch_bounds__((L / PTS) * W, 1) k_outer_inv(ClassParams p) {
   extern __shared__ double2 sm[];
-  constexpr int TC = L / PTS, G = W / 8;
+  constexpr int TC = L / PTS;
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   const int tiles = p.S1 / W;
   const long long total = (long long)p.nitems * tiles;
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__((L / PTS) * W, 1) k_outer_inv(ClassParams p) {
     __syncthreads();
     // one 8-column group of one row per thread: a real run and an imaginary run
     {
-      const int row = tid / G, g = tid % G;
+      const int row = tid % L, g = tid / L;
       double cre[8], cim[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) {

@@ -1,0 +1,431 @@
+// bc_pipe.cuh — persistent, double-buffered pass kernels.
+//
+// Same arithmetic as the passes in bc_kernels.cuh, restructured so that HBM
+// traffic overlaps the FP64 work: every CTA walks work units of its class in
+// a persistent loop and stages the next unit while it transforms the current
+// one.  Complex tiles arrive by TMA (cp.async.bulk.tensor, 128-byte swizzle,
+// completion on an mbarrier); the packing pass stages the limb words it needs
+// with cp.async.  Results leave by plain coalesced stores from registers.
+//
+// All items of a class sit in contiguous slabs (item i's buffer at i*M), so
+// one tensor map per slab serves the whole class.
+#pragma once
+#include "bc_async.cuh"
+#include "bc_kernels.cuh"
+
+namespace bc {
+
+// Tile width (columns) of an L-row pass tile: 2048 points, at least 8 columns.
+template <int L> struct PassTile {
+  static constexpr int W = (2048 / L) >= 8 ? 2048 / L : 8;
+  static constexpr int NT = (L / PTS) * W;
+  static constexpr int BOX_ROWS = L > 256 ? 256 : L;
+  static constexpr int HALVES = L / BOX_ROWS;
+  static constexpr unsigned BYTES = (unsigned)L * W * 16;
+  static constexpr int MINB = NT <= 256 ? 2 : 1;  // resident CTAs per SM the register budget allows for
+};
+
+__device__ __forceinline__ double2 *align1024(unsigned char *p) {
+  return reinterpret_cast<double2 *>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+
+// Issue the TMA loads of one L x W tile (W/8 boxes, each L rows of 8
+// complex; two boxes per column group when L = 512) into dst.
+template <int L, int W>
+__device__ __forceinline__ void tile_load_4d(double2 *dst, const CUtensorMap *map, uint64_t *bar, int col0, int c2,
+                                             int c3) {
+  using T = PassTile<L>;
+  mbar_expect_tx(bar, (unsigned)L * W * 16);
+#pragma unroll
+  for (int g = 0; g < W / 8; g++)
+#pragma unroll
+    for (int h = 0; h < T::HALVES; h++)
+      tma_load_4d(dst + g * L * 8 + h * T::BOX_ROWS * 8, map, bar, 2 * (col0 + 8 * g), h * T::BOX_ROWS, c2, c3);
+}
+template <int L, int W>
+__device__ __forceinline__ void tile_load_3d(double2 *dst, const CUtensorMap *map, uint64_t *bar, int col0, int c2) {
+  using T = PassTile<L>;
+  mbar_expect_tx(bar, (unsigned)L * W * 16);
+#pragma unroll
+  for (int g = 0; g < W / 8; g++)
+#pragma unroll
+    for (int h = 0; h < T::HALVES; h++)
+      tma_load_3d(dst + g * L * 8 + h * T::BOX_ROWS * 8, map, bar, 2 * (col0 + 8 * g), h * T::BOX_ROWS, c2);
+}
+
+// Twiddles of a thread's 8 points in a column pass, w^(m0 + i*dm) for
+// i = 0..7: two table lookups (base and step) and a running product, instead
+// of a two-level lookup per point.  `conj0` conjugates the base (the outer
+// pass's k = 0 term is e^{+2 pi i s/(4M)}).
+__device__ __forceinline__ void twiddle_run(const Tw2 &T, uint64_t m0, bool conj0, uint64_t dm, double2 (&w)[PTS]) {
+  double2 b = tw2_get(T, m0);
+  if (conj0) b.y = -b.y;
+  const double2 st = tw2_get(T, dm);
+  w[0] = b;
+#pragma unroll
+  for (int i = 1; i < PTS; i++) w[i] = cmul(w[i - 1], st);
+}
+
+// Outer pass: point (col, k1 = t + i*TC) takes e^{-2 pi i col(4 k1 - 1)/(4M)}.
+template <int TC>
+__device__ __forceinline__ void outer_twiddles(const Tw2 &T, int col, int t, double2 (&w)[PTS]) {
+  if (t == 0) twiddle_run(T, (uint64_t)col, true, (uint64_t)col * 4 * TC, w);
+  else twiddle_run(T, (uint64_t)col * (4 * t - 1), false, (uint64_t)col * 4 * TC, w);
+}
+
+// ------------------------------------------------------------------ middle (3 levels)
+// Units: (item, operand, block k1, column tile).  Map: 4-d view of a slab,
+// (2*Lr doubles, L2 rows, L1 blocks, items).
+template <int L, bool INV>
+__global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
+    k2_mid(ClassParams p, const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB) {
+  using T = PassTile<L>;
+  constexpr int W = T::W, TC = L / PTS;
+  extern __shared__ unsigned char smraw[];
+  __shared__ uint64_t bars[2];
+  double2 *buf[2];
+  buf[0] = align1024(smraw);
+  buf[1] = buf[0] + L * W;
+  const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const int tiles = p.Lr / W;
+  const int nops = (INV || p.sq) ? 1 : 2;
+  const long long per_op = (long long)p.L1 * tiles, per_item = nops * per_op;
+  const long long total = (long long)p.nitems * per_item;
+  auto decode = [&](long long u, int &item, int &op, int &blk, int &tile) {
+    item = (int)(u / per_item);
+    long long r = u % per_item;
+    op = (int)(r / per_op);
+    r %= per_op;
+    blk = (int)(r / tiles);
+    tile = (int)(r % tiles);
+  };
+  auto issue = [&](long long u, int st) {
+    int item, op, blk, tile;
+    decode(u, item, op, blk, tile);
+    fence_proxy_async_smem();
+    tile_load_4d<L, W>(buf[st], op ? &mB : &mA, &bars[st], tile * W, blk, item);
+  };
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned phase[2] = {0u, 0u};
+  int st = 0;
+  long long u = blockIdx.x;
+  if (tid == 0 && u < total) issue(u, 0);
+  for (; u < total; u += gridDim.x) {
+    const long long un = u + gridDim.x;
+    if (tid == 0 && un < total) issue(un, st ^ 1);
+    int item, op, blk, tile;
+    decode(u, item, op, blk, tile);
+    const ItemDesc &it = p.items[item];
+    const bool ok = mbar_wait(&bars[st], phase[st]);
+    phase[st] ^= 1;
+    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+    double2 *bf = buf[st];
+    double2 *g = (op ? it.bufB : it.bufA) + (uint64_t)blk * p.S1;
+    const int col = tile * W + s;
+    double2 v[PTS], w[PTS];
+    // e^{-2 pi i col k2/(L2 Lr)} = table index 4 L1 col k2 of the 4M table
+    twiddle_run(p.tw4M, (uint64_t)4 * p.L1 * col * t, false, (uint64_t)4 * p.L1 * col * TC, w);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      v[i] = bf[bidx<L>(t + i * TC, s)];
+      if (INV) v[i] = cmulc(v[i], w[i]);
+    }
+    __syncthreads();
+    block_fft<L, W, INV>(v, t, s, bf, p.twL2);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int k2 = t + i * TC;
+      g[(uint64_t)k2 * p.Lr + col] = INV ? v[i] : cmul(v[i], w[i]);
+    }
+    __syncthreads();
+    st ^= 1;
+  }
+}
+
+// ------------------------------------------------------------------ outer inverse
+// Units: (item, column tile).  Map: 3-d view of slab A, (2*S1, L1, items).
+template <int L>
+__global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_inv(ClassParams p, const __grid_constant__ CUtensorMap mA) {
+  using T = PassTile<L>;
+  constexpr int W = T::W, TC = L / PTS, G = W / 8;
+  extern __shared__ unsigned char smraw[];
+  __shared__ uint64_t bars[2];
+  double2 *buf[2];
+  buf[0] = align1024(smraw);
+  buf[1] = buf[0] + L * W;
+  const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const int tiles = p.S1 / W;
+  const long long total = (long long)p.nitems * tiles;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned phase[2] = {0u, 0u};
+  int st = 0;
+  long long u = blockIdx.x;
+  if (tid == 0 && u < total) {
+    fence_proxy_async_smem();
+    tile_load_3d<L, W>(buf[0], &mA, &bars[0], (int)(u % tiles) * W, (int)(u / tiles));
+  }
+  for (; u < total; u += gridDim.x) {
+    const long long un = u + gridDim.x;
+    if (tid == 0 && un < total) {
+      fence_proxy_async_smem();
+      tile_load_3d<L, W>(buf[st ^ 1], &mA, &bars[st ^ 1], (int)(un % tiles) * W, (int)(un / tiles));
+    }
+    const int item = (int)(u / tiles), tile = (int)(u % tiles);
+    const ItemDesc &it = p.items[item];
+    const bool ok = mbar_wait(&bars[st], phase[st]);
+    phase[st] ^= 1;
+    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+    double2 *bf = buf[st];
+    const int col = tile * W + s;
+    double2 v[PTS], w[PTS];
+    outer_twiddles<TC>(p.tw4M, col, t, w);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) v[i] = cmulc(bf[bidx<L>(t + i * TC, s)], w[i]);
+    __syncthreads();
+    block_fft<L, W, true>(v, t, s, bf, p.twL1);
+    double err = 0.0;
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int n1 = t + i * TC;
+      double2 z = cmul(v[i], __ldg(&p.pw_inv[n1]));
+      double re = rint(z.x), im = rint(z.y);
+      err = fmax(err, round_check(z, re, im));
+      bf[bidx<L>(n1, s)] = make_double2(re, im);
+    }
+    atomic_max_err(it.err, err);
+    __syncthreads();
+    {
+      // one 8-column group of one row per thread; consecutive lanes take
+      // consecutive rows of a group (distinct banks in the swizzled layout)
+      const int row = tid % L, gi = tid / L;
+      double cre[8], cim[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        double2 z = bf[bidx<L>(row, 8 * gi + q)];
+        cre[q] = z.x;
+        cim[q] = z.y;
+      }
+      const uint64_t n0 = (uint64_t)row * p.S1 + (uint64_t)tile * W + 8 * gi;
+      store_rec(&it.rec[n0 >> 3], make_run(cre, it.b));
+      store_rec(&it.rec[(n0 + p.M) >> 3], make_run(cim, it.b));
+    }
+    static_assert(PassTile<L>::NT == L * G, "one run pair per thread");
+    __syncthreads();
+    st ^= 1;
+  }
+}
+
+// ------------------------------------------------------------------ rows
+// Units: NR consecutive rows of the class's row space (items are contiguous
+// in the slab).  Map: 3-d view (16 doubles, Lr/8 lines, rows).  Buffer A is
+// refilled as soon as A's forward transform has left it, buffer B after the
+// inverse transform (which runs in B's buffer).
+constexpr int pow2_floor(int x) { return x >= 2 ? 2 * pow2_floor(x / 2) : 1; }
+
+template <int L> struct RowTile {
+  // rows per unit: a power of two (so units never straddle items, whose row
+  // counts are powers of two) with about 2048 points per operand
+  static constexpr int NR = pow2_floor(2048 / L > 0 ? 2048 / L : 1);
+  static constexpr int NT = (L / PTS) * NR;
+  static constexpr int LINES = L / 8;
+  // TMA boxes hold at most 256 lines: split a row into equal boxes
+  static constexpr int PARTS = (LINES + 255) / 256;
+  static constexpr int BOX_LINES = LINES / PARTS;
+  static_assert(BOX_LINES * PARTS == LINES && BOX_LINES % 8 == 0, "row split into whole swizzle atoms");
+  static_assert(PARTS == 1 || NR == 1, "split rows come one per unit");
+  static constexpr int MINB = NT <= 256 ? 2 : 1;
+};
+
+template <int L>
+__device__ __forceinline__ void rows_load(double2 *dst, const CUtensorMap *map, uint64_t *bar, long long row0) {
+  using R = RowTile<L>;
+  mbar_expect_tx(bar, (unsigned)R::NR * L * 16);
+  if (R::PARTS == 1) {
+    tma_load_3d(dst, map, bar, 0, 0, (int)row0);
+  } else {
+#pragma unroll
+    for (int h = 0; h < R::PARTS; h++) tma_load_3d(dst + h * R::BOX_LINES * 8, map, bar, 0, h * R::BOX_LINES, (int)row0);
+  }
+}
+
+template <int L, bool SQ>
+__global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
+    k2_rows(ClassParams p, const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB) {
+  using R = RowTile<L>;
+  constexpr int TC = L / PTS, NR = R::NR;
+  extern __shared__ unsigned char smraw[];
+  __shared__ uint64_t bars[2];  // 0: A buffer, 1: B buffer
+  double2 *bufA = align1024(smraw);
+  double2 *bufB = bufA + NR * L;
+  double2 *bufS = bufB + NR * L;  // A's spectrum while B is transformed
+  const int tid = threadIdx.x, rl = tid / TC, t = tid % TC;
+  const long long rows_item = p.M / L;
+  const long long total = (long long)p.nitems * rows_item / NR;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned phA = 0, phB = 0;
+  long long u = blockIdx.x;
+  if (tid == 0 && u < total) {
+    fence_proxy_async_smem();
+    rows_load<L>(bufA, &mA, &bars[0], u * NR);
+    if (!SQ) rows_load<L>(bufB, &mB, &bars[1], u * NR);
+  }
+  double2 *smA = bufA + rl * L, *smB = bufB + rl * L, *smS = bufS + rl * L;
+  for (; u < total; u += gridDim.x) {
+    const long long un = u + gridDim.x;
+    const long long grow = u * NR + rl;  // this thread's row in the class slab
+    const ItemDesc &it = p.items[grow / rows_item];
+    double2 *ra = it.bufA + (uint64_t)(grow % rows_item) * L;
+    double2 v[PTS];
+    bool ok = mbar_wait(&bars[0], phA);
+    phA ^= 1;
+    if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) v[i] = smA[ridx(t + i * TC)];
+    __syncthreads();
+    block_fft<L, 1, false>(v, t, 0, smA, p.twLr);
+    if (SQ) {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = cmul(v[i], v[i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) smS[ridx(t + i * TC)] = v[i];  // read back by this thread only
+    }
+    __syncthreads();
+    if (tid == 0 && un < total) {  // A's buffer is free: fetch the next rows of A
+      fence_proxy_async_smem();
+      rows_load<L>(bufA, &mA, &bars[0], un * NR);
+    }
+    if (!SQ) {
+      ok = mbar_wait(&bars[1], phB);
+      phB ^= 1;
+      if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = smB[ridx(t + i * TC)];
+      __syncthreads();
+      block_fft<L, 1, false>(v, t, 0, smB, p.twLr);
+#pragma unroll
+      for (int i = 0; i < PTS; i++) v[i] = cmul(smS[ridx(t + i * TC)], v[i]);
+    }
+    block_fft<L, 1, true>(v, t, 0, SQ ? smS : smB, p.twLr);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) ra[t + i * TC] = v[i];
+    __syncthreads();
+    if (!SQ && tid == 0 && un < total) {  // B's buffer is free after the inverse
+      fence_proxy_async_smem();
+      rows_load<L>(bufB, &mB, &bars[1], un * NR);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ outer forward (pack)
+// Units: (item, operand, column tile).  The limb words behind each tile row
+// (real and imaginary digit runs) are staged with cp.async one unit ahead;
+// digits are cut from shared memory.
+template <int L> struct PackTile {
+  static constexpr int W = PassTile<L>::W;
+  // words per staged row segment for widths up to 24 bits: the segment starts
+  // one word below the first digit's word and must hold the 64-bit window of
+  // the last digit (start offset < 64 bits, last window ends below 24W + 95)
+  static constexpr int SEGW = (24 * W + 95) / 32 + 1;
+  static constexpr int STAGE_WORDS = 2 * L * SEGW;
+};
+
+template <int L>
+__global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_fwd(ClassParams p) {
+  using T = PassTile<L>;
+  using K = PackTile<L>;
+  constexpr int W = T::W, TC = L / PTS, NT = T::NT, SEGW = K::SEGW;
+  extern __shared__ unsigned char smraw[];
+  double2 *tile = align1024(smraw);
+  uint32_t *stg = reinterpret_cast<uint32_t *>(tile + L * W);  // 2 stages of STAGE_WORDS
+  const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const int tiles = p.S1 / W;
+  const int nops = p.sq ? 1 : 2;
+  const long long per_item = (long long)nops * tiles;
+  const long long total = (long long)p.nitems * per_item;
+  // Row segment (n1, part) of tile tl starts one word below the word of digit
+  // j0 = n1*S1 + tl*W + part*M.  S1 and M are multiples of 32, so that word is
+  // n1*(S1 b/32) + part*(M b/32) + (tl*W*b >> 5) and digit j0 + s sits at bit
+  // 32 + (tl*W*b & 31) + s*b of the segment, for every row and both parts.
+  auto stage_copy = [&](long long u, int st) {
+    const int item = (int)(u / per_item), rem = (int)(u % per_item);
+    const int op = rem / tiles, tl = rem % tiles;
+    const ItemDesc &it = p.items[item];
+    const uint32_t *X = op ? it.B : it.A;
+    const long long XL = (long long)(op ? it.BL : it.AL);
+    const long long b = it.b;
+    const long long RW = (long long)p.S1 * b / 32, PW = (long long)p.M * b / 32;
+    const long long tw0 = ((long long)tl * W * b) >> 5;
+    uint32_t *dst = stg + st * K::STAGE_WORDS;
+    for (int idx = tid; idx < K::STAGE_WORDS; idx += NT) {
+      const int segi = idx / SEGW, k = idx - segi * SEGW;
+      const int part = segi >= L, row = segi - (part ? L : 0);
+      const long long w = row * RW + (part ? PW : 0) + tw0 - 1 + k;
+      const bool in = w >= 0 && w < XL;
+      cp_async4(dst + idx, X + (in ? w : 0), in ? 4 : 0);
+    }
+  };
+  long long u = blockIdx.x;
+  int st = 0;
+  if (u < total) stage_copy(u, 0);
+  cp_async_commit();
+  for (; u < total; u += gridDim.x) {
+    const long long un = u + gridDim.x;
+    if (un < total) stage_copy(un, st ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int item = (int)(u / per_item), rem = (int)(u % per_item);
+    const int op = rem / tiles, tl = rem % tiles;
+    const ItemDesc &it = p.items[item];
+    const unsigned long long nd = op ? it.ndB : it.ndA;
+    double2 *gbuf = op ? it.bufB : it.bufA;
+    const int b = it.b;
+    const uint32_t *seg = stg + st * K::STAGE_WORDS;
+    const int col = tl * W + s;
+    const unsigned rel = 32u + (unsigned)((tl * W * b) & 31) + (unsigned)(s * b);  // bit of digit j0+s
+    const unsigned wi = (rel - 1) >> 5, sh = (rel - 1) & 31;
+    const uint64_t mask = (1ull << b) - 1;
+    double2 v[PTS];
+#pragma unroll
+    for (int i = 0; i < PTS; i++) {
+      const int n1 = t + i * TC;
+      double d[2];
+#pragma unroll
+      for (int part = 0; part < 2; part++) {
+        const unsigned long long j = (unsigned long long)n1 * p.S1 + col + (part ? (unsigned long long)p.M : 0ull);
+        const uint32_t *rw = seg + (part * L + n1) * SEGW + wi;
+        const uint64_t win = ((uint64_t)rw[0] | ((uint64_t)rw[1] << 32)) >> sh;
+        const int64_t r = (int64_t)((win >> 1) & mask);
+        const int64_t top = (j + 1 >= nd) ? 0 : (r >> (b - 1));
+        d[part] = j < nd ? (double)(r - (top << b) + (int64_t)(win & 1)) : 0.0;
+      }
+      v[i] = cmul(make_double2(d[0], d[1]), __ldg(&p.pw_fwd[n1]));
+    }
+    block_fft<L, W, false>(v, t, s, tile, p.twL1);
+    double2 w[PTS];
+    outer_twiddles<TC>(p.tw4M, col, t, w);
+#pragma unroll
+    for (int i = 0; i < PTS; i++) gbuf[(uint64_t)(t + i * TC) * p.S1 + col] = cmul(v[i], w[i]);
+    __syncthreads();
+    st ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+}  // namespace bc

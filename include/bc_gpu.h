@@ -114,6 +114,10 @@ int bc_gpu_set_width_limit(size_t fft_points, int width);
 
 /* Force the width of subsequent products (0 = automatic); for error sweeps. */
 int bc_gpu_force_width(int width);
+/* Host-only check that every supported transform shape's launches are
+ * consistent (staged bytes equal awaited bytes, tiles cover rows); returns
+ * BC_OK or the first failing transform length.  No GPU needed. */
+int bc_gpu_check_shapes(void);
 /* Supported transform lengths in increasing order; returns the count. */
 int bc_gpu_lengths(size_t *out, int cap);
 /* Force transform length and width (0, 0 = automatic); for the autotuner. */

@@ -70,3 +70,9 @@ def test_width_table_monotone():
         w = bc.width_limit(M)
         assert w <= prev + 1  # non-increasing up to one-step noise
         prev = w
+
+
+def test_pipelined_launch_shapes_consistent():
+    # every supported length: TMA boxes deliver exactly the bytes each kernel
+    # waits for and tiles cover the rows (checked again before every launch)
+    assert bc._lib().bc_gpu_check_shapes() == 0

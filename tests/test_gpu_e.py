@@ -19,7 +19,9 @@ def _e(digits, per_call=False, env=None):
     with tempfile.TemporaryDirectory() as d:
         cmd = [bc.CLI, str(digits)] + (["--per-call"] if per_call else [])
         e = dict(os.environ, **(env or {}))
-        out = subprocess.run(cmd, cwd=d, check=True, capture_output=True, text=True, timeout=900, env=e).stdout
+        res = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=900, env=e)
+        assert res.returncode == 0, "bluecrunch %s failed (%d): %s" % (digits, res.returncode, res.stderr[-2000:])
+        out = res.stdout
         dec = open(os.path.join(d, "e.txt"), "rb").read()
         hexs = open(os.path.join(d, "e-hex.txt"), "rb").read()
     return hashlib.md5(dec).hexdigest(), hashlib.md5(hexs).hexdigest(), out
