@@ -60,9 +60,12 @@ bool shape_for(size_t M, Shape &s) {
       s.M = (int)M; s.L1 = L1; s.L2 = 1; s.Lr = (int)Lr; s.levels = 2; return true;
     }
   }
-  for (int i = (int)(sizeof(kRowLens) / sizeof(int)) - 1; i >= 0; i--) {
-    const size_t Lr = kRowLens[i];
-    if (Lr < 512 || M % Lr) continue;
+  // three levels: rows of about 1024 points keep the fused row pass free of
+  // spills with two rows per CTA; longer rows only when the outer passes run out
+  static const int kRowPref[] = {1024, 768, 1536, 512, 2048, 3072, 4096};
+  for (int Lri : kRowPref) {
+    const size_t Lr = (size_t)Lri;
+    if (M % Lr) continue;
     const size_t R = M / Lr;
     for (int L1 : kOuterLens) {
       if (R % L1) continue;
@@ -230,11 +233,20 @@ bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl,
   const size_t prod_words = (2 * M * (uint64_t)b) / 32;
   pl.nwords = std::min(CL, prod_words);
   pl.nruns = std::min((size_t)(2 * M / 8), (pl.nwords * 32 + 8 * b - 1) / (8 * b));
-  pl.ntiles = std::max<size_t>(1, (pl.nruns + CARRY_NT - 1) / CARRY_NT);
+  pl.ntiles = std::max<size_t>(1, (pl.nruns + CARRY_TILE_RUNS - 1) / CARRY_TILE_RUNS);
   return true;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// The packing pass stages limb words with 16-byte copies when the operand is
+// 16-byte aligned and every row segment of a tile shares one alignment
+// (S1*b/32 and M*b/32 multiples of 4 words); otherwise with 4-byte copies.
+int stage16_ok(const uint32_t *X, const Plan &pl) {
+  if (pl.shape.levels < 2 || ((uintptr_t)X & 15)) return 0;
+  const uint64_t S1 = (uint64_t)pl.shape.M / pl.shape.L1, b = (uint64_t)pl.b;
+  return ((S1 * b / 32) % 4 == 0 && ((uint64_t)pl.shape.M * b / 32) % 4 == 0) ? 1 : 0;
+}
 
 size_t work_bytes(const Plan &pl) {
   const size_t M = pl.shape.M;
@@ -796,6 +808,8 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
       it.flags = (unsigned int *)(base + off_flags) + i;
       it.b = pl.b;
       it.square = pl.square ? 1 : 0;
+      it.a16 = stage16_ok(it.A, pl);
+      it.b16 = stage16_ok(it.B, pl);
       k++;
     }
   }
@@ -1264,6 +1278,8 @@ extern "C" int bc_gpu_mul_noalloc(uint32_t *C, size_t CL, const uint32_t *A, siz
     it.flags = (unsigned int *)(nd.base + kNoAllocSlotsOff + 8);
     it.b = pl.b;
     it.square = square ? 1 : 0;
+    it.a16 = stage16_ok(it.A, pl);
+    it.b16 = stage16_ok(it.B, pl);
     ItemDesc *ddesc = (ItemDesc *)(nd.base + kNoAllocDescOff);
     unsigned int *ctr = (unsigned int *)(nd.base + kNoAllocSlotsOff + 12);
     // every call reuses the array: clear what the kernels expect to start at zero

@@ -49,6 +49,7 @@ struct ItemDesc {
   unsigned int *flags;
   int b;
   int square;
+  int a16, b16;                   // operand A / B starts on a 16-byte boundary
 };
 
 struct ClassParams {
@@ -338,6 +339,8 @@ __device__ __forceinline__ uint32_t block_scan_fn(uint32_t f, uint32_t *sw, uint
 // Decoupled lookback over tiles of CARRY_NT runs.  Tile status word:
 // 0 = not ready, (1<<30)|fn = aggregate, (2<<30)|(delta+1) = inclusive.
 constexpr int CARRY_NT = 256;
+constexpr int CARRY_RPT = 4;                            // runs per thread
+constexpr int CARRY_TILE_RUNS = CARRY_NT * CARRY_RPT;   // runs per lookback tile
 constexpr unsigned ST_AGG = 1u << 30, ST_INC = 2u << 30;
 constexpr int LOOKBACK_SPINS = 1 << 22;
 
@@ -375,21 +378,32 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
     }
     const ItemDesc &it = p.items[lo];
     const unsigned long long tile = unit - it.tile0;
-    const unsigned long long r = tile * CARRY_NT + tid;
+    // this thread's CARRY_RPT consecutive runs
+    const unsigned long long r0 = tile * CARRY_TILE_RUNS + (unsigned long long)tid * CARRY_RPT;
     const int nbits = 8 * it.b;
     const unsigned long long nrec = (unsigned long long)(2 * p.M) / 8;
-    U192 h = {{0, 0, 0}};
-    long long cself = 0;
-    uint32_t f = FN_ID;
-    if (r < it.nruns) {
-      RunRec rr = load_rec(&it.rec[r]);
-      h = rec_h(rr);
-      cself = rr.c;
-      const long long cprev = r ? load_rec(&it.rec[r - 1]).c : 0;
-      f = run_transfer(h, cprev, nbits);
+    U192 h[CARRY_RPT];
+    long long c[CARRY_RPT];
+    uint32_t f[CARRY_RPT];
+    uint32_t F = FN_ID;
+    long long cprev = (r0 > 0 && r0 < it.nruns) ? load_rec(&it.rec[r0 - 1]).c : 0;
+#pragma unroll
+    for (int q = 0; q < CARRY_RPT; q++) {
+      const unsigned long long r = r0 + q;
+      f[q] = FN_ID;
+      c[q] = 0;
+      h[q].w[0] = h[q].w[1] = h[q].w[2] = 0;
+      if (r < it.nruns) {
+        RunRec rr = load_rec(&it.rec[r]);
+        h[q] = rec_h(rr);
+        c[q] = rr.c;
+        f[q] = run_transfer(h[q], cprev, nbits);
+        cprev = rr.c;
+        F = fn_compose(F, f[q]);
+      }
     }
     uint32_t agg;
-    const uint32_t ex = block_scan_fn<CARRY_NT>(f, sw, &agg);
+    const uint32_t ex = block_scan_fn<CARRY_NT>(F, sw, &agg);
     if (tid == 0) {
       // A tile whose composed map is constant knows its carry out before its
       // carry in: it publishes that at once, and a lookback that meets such an
@@ -431,19 +445,32 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
       s_delta = din;
     }
     __syncthreads();
-    if (r < it.nruns) {
-      const int dprev = fn_apply(ex, s_delta);
-      const int dself = fn_apply(f, dprev);
-      u192_add_delta(h, dprev, nbits);
+    // carries into each run, then the words
+    int d = fn_apply(ex, s_delta);  // delta into run r0
+    int dout[CARRY_RPT];
+#pragma unroll
+    for (int q = 0; q < CARRY_RPT; q++) {
+      if (r0 + q < it.nruns) {
+        u192_add_delta(h[q], d, nbits);
+        d = fn_apply(f[q], d);
+      }
+      dout[q] = d;
+    }
+#pragma unroll
+    for (int q = 0; q < CARRY_RPT; q++) {
+      const unsigned long long r = r0 + q;
+      if (r >= it.nruns) break;
       U192 hn = {{0, 0, 0}};
-      if (r + 1 < nrec) {
+      if (q + 1 < CARRY_RPT && r + 1 < it.nruns) {
+        hn = h[q + 1];
+      } else if (r + 1 < nrec) {
         RunRec rn = load_rec(&it.rec[r + 1]);
         hn = rec_h(rn);
-        (void)u192_add_s64(hn, cself, nbits);
-        u192_add_delta(hn, dself, nbits);
+        (void)u192_add_s64(hn, c[q], nbits);
+        u192_add_delta(hn, dout[q], nbits);
       }
-      write_run_words(it.C, it.nwords, r, nbits, h, hn);
-      if (r + 1 == nrec && cself + dself != 0) atomicOr(it.flags, FLAG_TOPCARRY);
+      write_run_words(it.C, it.nwords, r, nbits, h[q], hn);
+      if (r + 1 == nrec && c[q] + dout[q] != 0) atomicOr(it.flags, FLAG_TOPCARRY);
     }
     // zero any words beyond the product (CL > product length)
     if (tile == 0) {

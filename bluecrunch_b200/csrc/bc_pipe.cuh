@@ -342,14 +342,18 @@ template <int L> struct PackTile {
   // one word below the first digit's word and must hold the 64-bit window of
   // the last digit (start offset < 64 bits, last window ends below 24W + 95)
   static constexpr int SEGW = (24 * W + 95) / 32 + 1;
-  static constexpr int STAGE_WORDS = 2 * L * SEGW;
+  // staged segment: up to 3 extra words in front so 16-byte chunks align
+  static constexpr int SEGW4 = (SEGW + 3 + 3) / 4 * 4;
+  static constexpr int STAGE_WORDS = 2 * L * SEGW4;
+  // the 64-bit window of the last digit (b <= 24, shift <= 3 words) stays inside
+  static_assert(SEGW4 >= ((158 + 24 * (W - 1)) >> 5) + 2, "staged segment too short");
 };
 
 template <int L>
 __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_fwd(ClassParams p) {
   using T = PassTile<L>;
   using K = PackTile<L>;
-  constexpr int W = T::W, TC = L / PTS, NT = T::NT, SEGW = K::SEGW;
+  constexpr int W = T::W, TC = L / PTS, NT = T::NT;
   extern __shared__ unsigned char smraw[];
   double2 *tile = align1024(smraw);
   uint32_t *stg = reinterpret_cast<uint32_t *>(tile + L * W);  // 2 stages of STAGE_WORDS
@@ -359,9 +363,14 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
   const long long per_item = (long long)nops * tiles;
   const long long total = (long long)p.nitems * per_item;
   // Row segment (n1, part) of tile tl starts one word below the word of digit
-  // j0 = n1*S1 + tl*W + part*M.  S1 and M are multiples of 32, so that word is
-  // n1*(S1 b/32) + part*(M b/32) + (tl*W*b >> 5) and digit j0 + s sits at bit
-  // 32 + (tl*W*b & 31) + s*b of the segment, for every row and both parts.
+  // j0 = n1*S1 + tl*W + part*M.  S1 and M are multiples of 128, so that word is
+  // n1*(S1 b/32) + part*(M b/32) + (tl*W*b >> 5), with the first two terms
+  // multiples of 4: every segment of a tile has the same alignment `dl` below
+  // a 16-byte boundary, and digit j0 + s sits at bit
+  // 32*(1 + dl) + (tl*W*b & 31) + s*b of its staged segment.
+  auto seg_shift = [&](int tl, int b, bool al16) -> int {
+    return al16 ? (int)((((long long)tl * W * b >> 5) - 1) & 3) : 0;
+  };
   auto stage_copy = [&](long long u, int st) {
     const int item = (int)(u / per_item), rem = (int)(u % per_item);
     const int op = rem / tiles, tl = rem % tiles;
@@ -369,15 +378,29 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     const uint32_t *X = op ? it.B : it.A;
     const long long XL = (long long)(op ? it.BL : it.AL);
     const long long b = it.b;
+    const bool al16 = op ? it.b16 : it.a16;
     const long long RW = (long long)p.S1 * b / 32, PW = (long long)p.M * b / 32;
-    const long long tw0 = ((long long)tl * W * b) >> 5;
+    const long long wbase = (((long long)tl * W * b) >> 5) - 1 - seg_shift(tl, (int)b, al16);
     uint32_t *dst = stg + st * K::STAGE_WORDS;
-    for (int idx = tid; idx < K::STAGE_WORDS; idx += NT) {
-      const int segi = idx / SEGW, k = idx - segi * SEGW;
-      const int part = segi >= L, row = segi - (part ? L : 0);
-      const long long w = row * RW + (part ? PW : 0) + tw0 - 1 + k;
-      const bool in = w >= 0 && w < XL;
-      cp_async4(dst + idx, X + (in ? w : 0), in ? 4 : 0);
+    if (al16) {
+      constexpr int CH = K::SEGW4 / 4, NCH = 2 * L * CH;
+      for (int idx = tid; idx < NCH; idx += NT) {
+        const int segi = idx / CH, k = idx - segi * CH;
+        const int part = segi >= L, row = segi - (part ? L : 0);
+        const long long w = row * RW + (part ? PW : 0) + wbase + 4 * k;  // multiple of 4
+        long long nv = XL - w;
+        nv = nv < 0 ? 0 : (nv > 4 ? 4 : nv);
+        if (w < 0) nv = 0;
+        cp_async16(dst + segi * K::SEGW4 + 4 * k, X + (nv ? w : 0), (int)nv * 4);
+      }
+    } else {
+      for (int idx = tid; idx < K::STAGE_WORDS; idx += NT) {
+        const int segi = idx / K::SEGW4, k = idx - segi * K::SEGW4;
+        const int part = segi >= L, row = segi - (part ? L : 0);
+        const long long w = row * RW + (part ? PW : 0) + wbase + k;
+        const bool in = w >= 0 && w < XL;
+        cp_async4(dst + idx, X + (in ? w : 0), in ? 4 : 0);
+      }
     }
   };
   long long u = blockIdx.x;
@@ -398,7 +421,9 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     const int b = it.b;
     const uint32_t *seg = stg + st * K::STAGE_WORDS;
     const int col = tl * W + s;
-    const unsigned rel = 32u + (unsigned)((tl * W * b) & 31) + (unsigned)(s * b);  // bit of digit j0+s
+    const bool al16 = op ? it.b16 : it.a16;
+    const unsigned rel = 32u * (1u + (unsigned)seg_shift(tl, b, al16)) + (unsigned)((tl * W * b) & 31) +
+                         (unsigned)(s * b);  // bit of digit j0+s in its staged segment
     const unsigned wi = (rel - 1) >> 5, sh = (rel - 1) & 31;
     const uint64_t mask = (1ull << b) - 1;
     double2 v[PTS];
@@ -409,7 +434,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
 #pragma unroll
       for (int part = 0; part < 2; part++) {
         const unsigned long long j = (unsigned long long)n1 * p.S1 + col + (part ? (unsigned long long)p.M : 0ull);
-        const uint32_t *rw = seg + (part * L + n1) * SEGW + wi;
+        const uint32_t *rw = seg + (part * L + n1) * K::SEGW4 + wi;
         const uint64_t win = ((uint64_t)rw[0] | ((uint64_t)rw[1] << 32)) >> sh;
         const int64_t r = (int64_t)((win >> 1) & mask);
         const int64_t top = (j + 1 >= nd) ? 0 : (r >> (b - 1));
