@@ -63,52 +63,105 @@ def peaks():
 
 
 class Clocks:
-    """Samples nvidia-smi during the timed region."""
+    """Samples SM clock, power and clock-event reasons every 10 ms during the
+    timed region through NVML (read-only queries), falling back to
+    `nvidia-smi -lms 200`.  The first sample is taken before __enter__
+    returns, so even a short timed region is covered."""
 
-    def __init__(self, index=0):
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+    def __init__(self, index=0, period_s=0.01):
         self.index = index
-        self.rows = []
+        self.period = period_s
+        self.rows = []  # (sm_mhz, max_mhz, watts, set of reason names)
         self.proc = None
+        self.stop = threading.Event()
+        self.thread = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [x for x in vis.split(",") if x.strip().isdigit()]
+            phys = int(ids[self.index]) if self.index < len(ids) else self.index
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(phys)
+
+    def _nvml_loop(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while True:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                w = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), w, {n for n, b in bits.items() if rs & b}))
+            except Exception:
+                pass
+            if self.stop.wait(self.period):
+                break
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            nv, h = self._nvml_handle()
+            self.source = "nvml 10 ms"
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
             self.thread.start()
-        except OSError:
-            self.proc = None
+        except Exception:
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.source = "nvidia-smi 200 ms"
+                self.thread = threading.Thread(target=self._smi_read, daemon=True)
+                self.thread.start()
+            except OSError:
+                self.proc = None
+        t0 = time.perf_counter()
+        while self.thread is not None and not self.rows and time.perf_counter() - t0 < 3.0:
+            time.sleep(0.005)
         return self
 
-    def _read(self):
+    def _smi_read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            try:
+                reasons = {n for i, n in enumerate(self.NAMES) if len(r) > 5 + i and r[5 + i].lower().startswith("active")}
+                self.rows.append((float(r[1]), float(r[2]), float(r[3]), reasons))
+            except (ValueError, IndexError):
+                pass
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         reasons = set()
         for r in self.rows:
-            for i, n in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+            reasons |= r[3]
+        return {"sm_mhz": float(np.median([r[0] for r in self.rows])), "sm_max_mhz": max(r[1] for r in self.rows),
+                "power_w_median": round(float(np.median([r[2] for r in self.rows])), 1),
+                "reasons": sorted(reasons), "samples": len(self.rows), "source": self.source}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -160,6 +213,79 @@ def reference_arm(args):
                                    "%d threads, %d timed multiplies of 2^20 x 2^20 limbs" % (threads, K)},
         "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+# ---------------------------------------------------------------- batched products
+def batched_workload(n=8192, lo=128, hi=262144, seed=0xB1C0FFEE, sibling=False):
+    """n independent products; AL, BL log-uniform in [lo, hi] limbs (or BL =
+    AL*U(0.875, 1.125) for the sibling variant that mimics a splitting level)."""
+    rng = np.random.default_rng(seed)
+    al = np.exp(rng.uniform(np.log(lo), np.log(hi), n)).astype(np.int64)
+    if sibling:
+        bl = np.maximum(1, (al * rng.uniform(0.875, 1.125, n)).astype(np.int64))
+    else:
+        bl = np.exp(rng.uniform(np.log(lo), np.log(hi), n)).astype(np.int64)
+    return al, bl
+
+
+def run_batched(bc, torch, stream, n=8192, sibling=False, per_call=True, reps=2):
+    import oracle
+    al, bl = batched_workload(n, sibling=sibling)
+    tot = int(al.sum() + bl.sum())
+    pool = torch.from_numpy(oracle.random_limbs(0x5EED ^ n, tot).view(np.int32)).cuda()
+    out = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    descs = (bc.MulDesc * n)()
+    offs = np.concatenate([[0], np.cumsum(al + bl)])
+    base_in, base_out = pool.data_ptr(), out.data_ptr()
+    nbytes = 0
+    for i in range(n):
+        a0, b0 = int(offs[i]), int(offs[i] + al[i])
+        CL = int(al[i] + bl[i])
+        descs[i] = bc.MulDesc(base_out + 4 * int(offs[i]), CL, base_in + 4 * a0, int(al[i]),
+                              base_in + 4 * b0, int(bl[i]))
+        p = bc.plan(int(al[i]), int(bl[i]), CL)
+        nbytes += alg_bytes(int(al[i]), int(bl[i]), CL, bc.width_limit(p["fft_points"]), False)
+    bc.mul_batch_desc(descs, n)  # warm
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        st = bc.mul_batch_desc(descs, n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = e0.elapsed_time(e1) / reps
+    # spot check: modular check of a few items against the oracle
+    R = oracle.restated()
+    pool_h = pool.cpu().numpy().view(np.uint32)
+    out_h = out.cpu().numpy().view(np.uint32)
+    ok = True
+    for i in np.random.default_rng(1).choice(n, 16, replace=False):
+        a = pool_h[offs[i]:offs[i] + al[i]]
+        b = pool_h[offs[i] + al[i]:offs[i + 1]]
+        c = out_h[offs[i]:offs[i + 1]]
+        ok &= R.modcheck(c, a, b, 2)
+    res = {"items": n, "sibling": sibling, "total_limbs_in": tot, "classes": st["classes"],
+           "launches_per_batch": st["launches"], "batched_ms": round(batched_ms, 3),
+           "batched_GBps": round(nbytes / (batched_ms * 1e-3) / 1e9, 1),
+           "products_per_s": round(n / (batched_ms * 1e-3), 1), "modcheck_sample_ok": bool(ok)}
+    if per_call:
+        out.zero_()
+        lib = bc._lib()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(n):
+            d = descs[i]
+            rc = lib.bc_gpu_mul(d.C, d.CL, d.A, d.AL, d.B, d.BL, None)
+            if rc:
+                raise bc.BcError(rc)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        per_ms = e0.elapsed_time(e1)
+        res.update({"per_call_ms": round(per_ms, 3), "speedup_batched_vs_per_call": round(per_ms / batched_ms, 2)})
+    del pool, out
+    torch.cuda.empty_cache()
+    return res
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -313,6 +439,15 @@ def gpu_arm(args):
             except Exception as exc:  # report, keep going
                 sweep.append({"log2": lg, "ratio": ratio, "square": sq, "error": str(exc)[:200]})
 
+    # ---- batched uneven products (8192 per launch sequence) vs per-call launches
+    batched = []
+    if not args.no_batched and rank == 0:
+        for sib in (False, True):
+            try:
+                batched.append(run_batched(bc, torch, stream, n=args.batch_items, sibling=sib))
+            except Exception as exc:
+                batched.append({"sibling": sib, "error": str(exc)[:300]})
+
     # ---- CPU baseline: the reference multiply on the host cores, bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -352,6 +487,7 @@ def gpu_arm(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "sweep": sweep,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -368,6 +504,8 @@ def main():
     ap.add_argument("--log2", type=int, default=HEADLINE_LOG2)
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-items", type=int, default=8192)
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -75,6 +75,7 @@ GPU_SYMBOLS = {
     "bc_gpu_mul": (ctypes.c_int, [ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz,
                                   ctypes.POINTER(MulStats)]),
     "bc_gpu_mul_batch": (ctypes.c_int, [ctypes.POINTER(MulDesc), _sz, ctypes.POINTER(BatchStats)]),
+    "bc_gpu_mul_batch_flags": (ctypes.c_int, [ctypes.POINTER(MulDesc), _sz, ctypes.c_uint, ctypes.POINTER(BatchStats)]),
     "bc_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p]),
     "bc_gpu_plan": (ctypes.c_int, [_sz, _sz, _sz, ctypes.c_int, ctypes.POINTER(PlanInfo)]),
     "bc_gpu_width_limit": (ctypes.c_int, [_sz]),

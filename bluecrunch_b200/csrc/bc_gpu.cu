@@ -681,7 +681,8 @@ int pinned_reserve(PinnedStage &ps, size_t bytes) {
 
 // Run one attempt over `works` (none done yet).  Fills err/flags and copies
 // out the products that pass the rounding check.
-int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st) {
+int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st, unsigned flags_in) {
+  const bool all_host = flags_in & BC_BATCH_HOST_OPERANDS;
   const size_t nw = works.size();
   // ---- classes (M, square); items of a class get contiguous slabs
   std::map<std::pair<size_t, bool>, std::vector<size_t>> classes;
@@ -697,20 +698,24 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   for (size_t i = 0; i < nw; i++) {
     const bc_mul_desc &d = items[works[i]->idx];
     const Plan &pl = works[i]->pl;
-    hostA[i] = pl.AL && !is_device_ptr(d.A);
-    hostB[i] = !pl.square && pl.BL && !is_device_ptr(d.B);
-    runs[i].hostC = !is_device_ptr(d.C);
+    hostA[i] = pl.AL && (all_host || !is_device_ptr(d.A));
+    hostB[i] = !pl.square && pl.BL && (all_host || !is_device_ptr(d.B));
+    runs[i].hostC = all_host || !is_device_ptr(d.C);
     runs[i].stagedC = !runs[i].hostC && (overlaps(d.C, d.CL * 4, d.A, d.AL * 4) || overlaps(d.C, d.CL * 4, d.B, d.BL * 4));
     slots[i].off_dA = off; if (hostA[i]) off += align256(pl.AL * 4);
     slots[i].off_dB = off; if (hostB[i]) off += align256(pl.BL * 4);
-    slots[i].off_dC = off; if (runs[i].hostC || runs[i].stagedC) off += align256(d.CL * 4);
     if (hostA[i] && pl.AL * 4 <= kStageItemMax) { pin_in_off[i] = stage_in; stage_in += align256(pl.AL * 4); }
     if (hostB[i] && pl.BL * 4 <= kStageItemMax) { pin_inB_off[i] = stage_in; stage_in += align256(pl.BL * 4); }
     if (runs[i].hostC && d.CL * 4 <= kStageItemMax) { pin_out_off[i] = stage_out; stage_out += align256(d.CL * 4); }
+    slots[i].off_dC = off;
+    if ((runs[i].hostC && pin_out_off[i] == SIZE_MAX) || runs[i].stagedC) off += align256(d.CL * 4);
   }
-  // the staged inputs sit contiguously in the arena so one copy moves them
+  // staged inputs and staged outputs each sit contiguously in the arena, in
+  // the order of their pinned host copies, so one copy moves each way
   const size_t off_stage_in = off;
   off += align256(stage_in);
+  const size_t off_stage_out = off;
+  off += align256(stage_out);
   struct ClassSlab { size_t offA = 0, offB = 0; };
   std::map<std::pair<size_t, bool>, ClassSlab> slab;
   for (auto &c : classes) {
@@ -770,7 +775,8 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
       CK(cudaMemcpyAsync((void *)runs[i].dB, d.B, pl.BL * 4, cudaMemcpyHostToDevice, g.stream));
       st->h2d_bytes += pl.BL * 4;
     }
-    runs[i].dC = (runs[i].hostC || runs[i].stagedC) ? (uint32_t *)(base + slots[i].off_dC) : d.C;
+    if (pin_out_off[i] != SIZE_MAX) runs[i].dC = (uint32_t *)(base + off_stage_out + pin_out_off[i]);
+    else runs[i].dC = (runs[i].hostC || runs[i].stagedC) ? (uint32_t *)(base + slots[i].off_dC) : d.C;
   }
   CK(cudaMemsetAsync(base + off_err, 0, zero_end - off_err, g.stream));
 
@@ -879,17 +885,20 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     if (!ok[i]) continue;
     if (runs[i].hostC) {
       if (pin_out_off[i] != SIZE_MAX) {
-        CK(cudaMemcpyAsync(g_pin_out.p + pin_out_off[i], runs[i].dC, d.CL * 4, cudaMemcpyDeviceToHost, g.stream));
-        staged_out = true;
+        staged_out = true;  // one copy of the whole staged span below
       } else {
         CK(cudaMemcpyAsync(d.C, runs[i].dC, d.CL * 4, cudaMemcpyDeviceToHost, g.stream));
+        st->d2h_bytes += d.CL * 4;
       }
-      st->d2h_bytes += d.CL * 4;
       copies = true;
     } else if (runs[i].stagedC) {
       CK(cudaMemcpyAsync(d.C, runs[i].dC, d.CL * 4, cudaMemcpyDeviceToDevice, g.stream));
       copies = true;
     }
+  }
+  if (staged_out) {
+    CK(cudaMemcpyAsync(g_pin_out.p, base + off_stage_out, stage_out, cudaMemcpyDeviceToHost, g.stream));
+    st->d2h_bytes += stage_out;
   }
   if (copies) CK(cudaStreamSynchronize(g.stream));
   if (staged_out)
@@ -898,7 +907,8 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   return BC_OK;
 }
 
-int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Plan *first_plan = nullptr) {
+int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Plan *first_plan = nullptr,
+                     unsigned flags = 0) {
   if (!g.init) return fail(BC_ERR_NOT_INIT);
   if (n && !items) return fail(BC_ERR_INVALID);
   auto t0 = std::chrono::steady_clock::now();
@@ -911,7 +921,7 @@ int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Pla
     if (d.CL == 0) continue;
     const bool zero = d.AL == 0 || d.BL == 0;
     if (zero) {
-      if (is_device_ptr(d.C)) CK(cudaMemsetAsync(d.C, 0, d.CL * 4, g.stream));
+      if (!(flags & BC_BATCH_HOST_OPERANDS) && is_device_ptr(d.C)) CK(cudaMemsetAsync(d.C, 0, d.CL * 4, g.stream));
       else memset(d.C, 0, d.CL * 4);
       continue;
     }
@@ -941,7 +951,7 @@ int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Pla
         i1++;
       }
       std::vector<Work *> chunk(todo.begin() + i0, todo.begin() + i1);
-      int r = run_attempt(items, chunk, st);
+      int r = run_attempt(items, chunk, st, flags);
       if (r) return r;
       i0 = i1;
     }
@@ -1048,6 +1058,14 @@ int bc_gpu_mul_batch(const bc_mul_desc *items, size_t n, bc_batch_stats *stats) 
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   bc_batch_stats st{};
   int r = mul_batch_locked(items, n, &st);
+  if (stats) *stats = st;
+  return r;
+}
+
+int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, bc_batch_stats *stats) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  bc_batch_stats st{};
+  int r = mul_batch_locked(items, n, &st, nullptr, flags);
   if (stats) *stats = st;
   return r;
 }

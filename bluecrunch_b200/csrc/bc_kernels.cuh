@@ -1,20 +1,23 @@
-// bc_kernels.cuh — pass kernels of the exact FFT multiply (sm_100a).
+// bc_kernels.cuh — shared pieces of the exact FFT multiply (sm_100a): item
+// and class descriptors, rounding check, the carry kernel and the one-CTA
+// kernel for short transforms.
 //
 // A product class has complex length M = L1 * S1 (two levels, S1 = Lr) or
 // M = L1 * L2 * Lr (three levels).  Point n of operand X holds the balanced
 // digits n and n+M weighted by e^{i pi n/(2M)}.  Passes (one launch each,
-// every launch covers all items of the class):
+// every launch covers all items of the class; the pass kernels are in
+// bc_pipe.cuh):
 //
-//   k_outer_fwd   digits -> pre-weight -> L1-point DFT down each column of the
+//   k2_outer_fwd  digits -> pre-weight -> L1-point DFT down each column of the
 //                 L1 x S1 matrix -> twiddle e^{-2 pi i s(4k1-1)/(4M)} (the
 //                 column's weight factor folded in) -> buffer
-//   k_mid<false>  (3 levels) L2-point DFT down columns of each L2 x Lr block,
+//   k2_mid<L,0>   (3 levels) L2-point DFT down columns of each L2 x Lr block,
 //                 twiddle e^{-2 pi i s k2/(L2 Lr)}
-//   k_rows        per row of Lr points: forward DFT of A and B, pointwise
+//   k2_rows       per row of Lr points: forward DFT of A and B, pointwise
 //                 product (or square), inverse DFT — the spectrum never
 //                 leaves the chip
-//   k_mid<true>   (3 levels) inverse of k_mid
-//   k_outer_inv   conjugate twiddle -> inverse L1-point DFT -> un-weight and
+//   k2_mid<L,1>   (3 levels) inverse of k2_mid<L,0>
+//   k2_outer_inv  conjugate twiddle -> inverse L1-point DFT -> un-weight and
 //                 1/M -> round (max |x - round(x)| recorded) -> run records:
 //                 8 consecutive coefficients -> (H, C), value H + C*2^{8b}
 //   k_carry       decoupled-lookback scan of run carries -> output words
@@ -94,124 +97,6 @@ __device__ __forceinline__ void atomic_max_err(unsigned long long *p, double e) 
   if ((threadIdx.x & 31) == 0 && bits) atomicMax(p, bits);
 }
 
-// ------------------------------------------------------------------ outer fwd
-template <int L, int W>
-__global__ void __launch_bounds__((L / PTS) * W, 1) k_outer_fwd(ClassParams p) {
-  extern __shared__ double2 sm[];
-  constexpr int TC = L / PTS;
-  const int tid = threadIdx.x, s = tid % W, t = tid / W;
-  const int tiles = p.S1 / W;
-  const long long total = (long long)p.nitems * 2 * tiles;
-  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
-    const int item = (int)(unit / (2 * tiles));
-    const int rem = (int)(unit % (2 * tiles));
-    const int op = rem / tiles, tile = rem % tiles;
-    const ItemDesc &it = p.items[item];
-    if (op == 1 && it.square) continue;
-    const uint32_t *X = op ? it.B : it.A;
-    const unsigned long long XL = op ? it.BL : it.AL, nd = op ? it.ndB : it.ndA;
-    double2 *buf = op ? it.bufB : it.bufA;
-    const int col = tile * W + s;
-    double2 v[PTS];
-#pragma unroll
-    for (int i = 0; i < PTS; i++) {
-      const int n1 = t + i * TC;
-      const uint64_t n = (uint64_t)n1 * p.S1 + col;
-      double2 z = make_double2(digit_at(X, XL, it.b, n, nd), digit_at(X, XL, it.b, n + p.M, nd));
-      v[i] = cmul(z, __ldg(&p.pw_fwd[n1]));
-    }
-    block_fft<L, W, false>(v, t, s, sm, p.twL1);
-#pragma unroll
-    for (int i = 0; i < PTS; i++) {
-      const int k1 = t + i * TC;
-      buf[(uint64_t)k1 * p.S1 + col] = cmul(v[i], outer_tw(p.tw4M, col, k1));
-    }
-  }
-}
-
-// ------------------------------------------------------------------ middle (3 levels)
-template <int L, int W, bool INV>
-__global__ void __launch_bounds__((L / PTS) * W, 1) k_mid(ClassParams p) {
-  extern __shared__ double2 sm[];
-  constexpr int TC = L / PTS;
-  const int tid = threadIdx.x, s = tid % W, t = tid / W;
-  const int tiles = p.Lr / W;
-  const int nops = INV ? 1 : 2;
-  const long long per_item = (long long)nops * p.L1 * tiles;
-  const long long total = (long long)p.nitems * per_item;
-  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
-    const int item = (int)(unit / per_item);
-    long long rem = unit % per_item;
-    const int op = (int)(rem / ((long long)p.L1 * tiles));
-    rem %= (long long)p.L1 * tiles;
-    const int blk = (int)(rem / tiles), tile = (int)(rem % tiles);
-    const ItemDesc &it = p.items[item];
-    if (op == 1 && it.square) continue;
-    double2 *buf = (op ? it.bufB : it.bufA) + (uint64_t)blk * p.S1;
-    const int col = tile * W + s;
-    double2 v[PTS];
-    if (!INV) {
-#pragma unroll
-      for (int i = 0; i < PTS; i++) v[i] = buf[(uint64_t)(t + i * TC) * p.Lr + col];
-      block_fft<L, W, false>(v, t, s, sm, p.twL2);
-#pragma unroll
-      for (int i = 0; i < PTS; i++) {
-        const int k2 = t + i * TC;
-        const double2 w = tw2_get(p.tw4M, (uint64_t)4 * p.L1 * ((uint64_t)col * k2));
-        buf[(uint64_t)k2 * p.Lr + col] = cmul(v[i], w);
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < PTS; i++) {
-        const int k2 = t + i * TC;
-        const double2 w = tw2_get(p.tw4M, (uint64_t)4 * p.L1 * ((uint64_t)col * k2));
-        v[i] = cmulc(buf[(uint64_t)k2 * p.Lr + col], w);
-      }
-      block_fft<L, W, true>(v, t, s, sm, p.twL2);
-#pragma unroll
-      for (int i = 0; i < PTS; i++) buf[(uint64_t)(t + i * TC) * p.Lr + col] = v[i];
-    }
-  }
-}
-
-// ------------------------------------------------------------------ rows
-// NR rows of Lr points per CTA; forward A (and B), product, inverse, in place
-// in bufA.
-template <int L, int NR, bool SQ>
-__global__ void __launch_bounds__((L / PTS) * NR, 1) k_rows(ClassParams p) {
-  extern __shared__ double2 sm[];
-  constexpr int TC = L / PTS, ROWE = TileSmem<L, 1>::elems;
-  const int tid = threadIdx.x, rl = tid / TC, t = tid % TC;
-  double2 *smr = sm + rl * ROWE;
-  const int rows = p.M / L;
-  const int groups = rows / NR;
-  const long long total = (long long)p.nitems * groups;
-  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
-    const int item = (int)(unit / groups);
-    const int row = (int)(unit % groups) * NR + rl;
-    const ItemDesc &it = p.items[item];
-    double2 *ra = it.bufA + (uint64_t)row * L;
-    double2 va[PTS], v[PTS];
-#pragma unroll
-    for (int i = 0; i < PTS; i++) va[i] = ra[t + i * TC];
-    block_fft<L, 1, false>(va, t, 0, smr, p.twLr);
-    if (SQ) {
-#pragma unroll
-      for (int i = 0; i < PTS; i++) v[i] = cmul(va[i], va[i]);
-    } else {
-      const double2 *rb = it.bufB + (uint64_t)row * L;
-#pragma unroll
-      for (int i = 0; i < PTS; i++) v[i] = rb[t + i * TC];
-      block_fft<L, 1, false>(v, t, 0, smr, p.twLr);
-#pragma unroll
-      for (int i = 0; i < PTS; i++) v[i] = cmul(va[i], v[i]);
-    }
-    block_fft<L, 1, true>(v, t, 0, smr, p.twLr);
-#pragma unroll
-    for (int i = 0; i < PTS; i++) ra[t + i * TC] = v[i];
-  }
-}
-
 // ------------------------------------------------------------------ runs
 // 8 consecutive rounded coefficients c_u (exact integers held in doubles) ->
 // H = sum (bits of the running carry) and C = final signed carry.
@@ -248,53 +133,6 @@ __device__ __forceinline__ RunRec load_rec(const RunRec *src) {
   RunRec r;
   r.h0 = a.x; r.h1 = a.y; r.h2 = b.x; r.c = (long long)b.y;
   return r;
-}
-
-// ------------------------------------------------------------------ outer inv
-template <int L, int W>
-__global__ void __launch_bounds__((L / PTS) * W, 1) k_outer_inv(ClassParams p) {
-  extern __shared__ double2 sm[];
-  constexpr int TC = L / PTS;
-  const int tid = threadIdx.x, s = tid % W, t = tid / W;
-  const int tiles = p.S1 / W;
-  const long long total = (long long)p.nitems * tiles;
-  for (long long unit = blockIdx.x; unit < total; unit += gridDim.x) {
-    const int item = (int)(unit / tiles), tile = (int)(unit % tiles);
-    const ItemDesc &it = p.items[item];
-    const int col = tile * W + s;
-    double2 v[PTS];
-#pragma unroll
-    for (int i = 0; i < PTS; i++) {
-      const int k1 = t + i * TC;
-      v[i] = cmulc(it.bufA[(uint64_t)k1 * p.S1 + col], outer_tw(p.tw4M, col, k1));
-    }
-    block_fft<L, W, true>(v, t, s, sm, p.twL1);
-    double err = 0.0;
-#pragma unroll
-    for (int i = 0; i < PTS; i++) {
-      const int n1 = t + i * TC;
-      double2 z = cmul(v[i], __ldg(&p.pw_inv[n1]));
-      double re = rint(z.x), im = rint(z.y);
-      err = fmax(err, round_check(z, re, im));
-      sm[sidx<L, W>(n1, s)] = make_double2(re, im);
-    }
-    atomic_max_err(it.err, err);
-    __syncthreads();
-    // one 8-column group of one row per thread: a real run and an imaginary run
-    {
-      const int row = tid % L, g = tid / L;
-      double cre[8], cim[8];
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        double2 z = sm[sidx<L, W>(row, 8 * g + u)];
-        cre[u] = z.x; cim[u] = z.y;
-      }
-      const uint64_t n0 = (uint64_t)row * p.S1 + (uint64_t)tile * W + 8 * g;
-      store_rec(&it.rec[n0 >> 3], make_run(cre, it.b));
-      store_rec(&it.rec[(n0 + p.M) >> 3], make_run(cim, it.b));
-    }
-    __syncthreads();
-  }
 }
 
 // ------------------------------------------------------------------ scan helper

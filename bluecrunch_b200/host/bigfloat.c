@@ -268,39 +268,58 @@ void bigfloat_mul(bigfloat_t t, const bigfloat_t a, const bigfloat_t b, size_t p
 /* Batch of bigfloat_mul: small products on the host, the rest in one
  * bc_gpu_mul_batch call.  Each result is what bigfloat_mul would produce. */
 void bigfloat_mul_batch(bigfloat_mul_item *items, size_t n) {
+  /* 1: operands, targets and which products go to the GPU (serial: cheap) */
   bc_gpu_item *g = (bc_gpu_item *)bc_xmalloc((n ? n : 1) * sizeof(bc_gpu_item));
+  bc_operand *ops = (bc_operand *)bc_xmalloc((n ? 2 * n : 2) * sizeof(bc_operand));
+  char *kind = (char *)bc_xmalloc(n ? n : 1);  /* 0 zero, 1 host, 2 gpu */
   size_t ng = 0;
   for (size_t i = 0; i < n; i++) {
     _bigfloat_struct *t = items[i].target;
     const _bigfloat_struct *a = items[i].a, *b = items[i].b;
     if (bigfloat_iszero(a) || bigfloat_iszero(b)) {
       bigfloat_zero(t);
+      kind[i] = 0;
       continue;
     }
-    bc_operand oa, ob;
-    bc_mul_operands(a, b, items[i].p, &oa, &ob);
-    const size_t CL = oa.L + ob.L;
+    bc_operand *oa = &ops[2 * i], *ob = &ops[2 * i + 1];
+    bc_mul_operands(a, b, items[i].p, oa, ob);
+    const size_t CL = oa->L + ob->L;
     uint32_t *c = (uint32_t *)bc_xmalloc(CL * sizeof(uint32_t));
-    if (CL == 2) {
-      uint64_t r = (uint64_t)oa.T[0] * ob.T[0];
-      c[0] = (uint32_t)r;
-      c[1] = (uint32_t)(r >> 32);
-    } else if (CL < BC_SMALL_PRODUCT_LIMBS) {
-      bc_small_mul(c, CL, oa.T, oa.L, ob.T, ob.L);
-    } else {
-      g[ng].C = c; g[ng].CL = CL; g[ng].A = oa.T; g[ng].AL = oa.L; g[ng].B = ob.T; g[ng].BL = ob.L;
+    kind[i] = (CL == 2 || CL < BC_SMALL_PRODUCT_LIMBS) ? 1 : 2;
+    if (kind[i] == 2) {
+      g[ng].C = c; g[ng].CL = CL; g[ng].A = oa->T; g[ng].AL = oa->L; g[ng].B = ob->T; g[ng].BL = ob->L;
       ng++;
     }
-    /* fields are set now; the limbs of GPU items arrive below */
     free(t->coef);
     t->coef = c;
     t->sign = a->sign == b->sign;
-    t->exp = oa.exp + ob.exp;
+    t->exp = oa->exp + ob->exp;
     t->len = CL;
   }
-  if (ng) bc_host_gpu_batch(g, ng);
+  /* 2: GPU products in one batch while host threads do the small ones */
+  long nn = (long)n;
+#pragma omp parallel
+  {
+#pragma omp single nowait
+    if (ng) bc_host_gpu_batch(g, ng);
+#pragma omp for schedule(dynamic, 256)
+    for (long i = 0; i < nn; i++) {
+      if (kind[i] != 1) continue;
+      _bigfloat_struct *t = items[i].target;
+      const bc_operand *oa = &ops[2 * i], *ob = &ops[2 * i + 1];
+      if (t->len == 2) {
+        uint64_t r = (uint64_t)oa->T[0] * ob->T[0];
+        t->coef[0] = (uint32_t)r;
+        t->coef[1] = (uint32_t)(r >> 32);
+      } else {
+        bc_small_mul(t->coef, t->len, oa->T, oa->L, ob->T, ob->L);
+      }
+    }
+  }
   for (size_t i = 0; i < n; i++)
-    if (items[i].target->len) trim_product(items[i].target);
+    if (kind[i]) trim_product(items[i].target);
+  free(kind);
+  free(ops);
   free(g);
 }
 

@@ -29,8 +29,9 @@ int main(int argc, char *argv[]) {
   if (getenv("BC_STATS")) {
     bigfloat_mul_counters c;
     bigfloat_get_counters(&c);
-    printf("GPU products: %zu in %zu calls, %.3f s inside GPU calls; host small products: %zu\n",
-           c.gpu_products, c.gpu_calls, c.gpu_seconds, c.small_products);
+    printf("GPU products: %zu in %zu calls, %.3f s inside GPU calls (%.3f s kernels of batches); "
+           "host small products: %zu\n",
+           c.gpu_products, c.gpu_calls, c.gpu_seconds, c.gpu_kernel_seconds, c.small_products);
   }
   return rc ? 1 : 0;
 }

@@ -23,6 +23,7 @@
 static pthread_once_t g_once = PTHREAD_ONCE_INIT;
 static int g_init_rc = 0;
 static bigfloat_mul_counters g_cnt;
+static unsigned long long g_device_us;
 static pthread_mutex_t g_cnt_mu = PTHREAD_MUTEX_INITIALIZER;
 
 void *bc_xmalloc(size_t n) {
@@ -144,8 +145,9 @@ void bc_host_gpu_batch(bc_gpu_item *items, size_t n) {
   }
   bc_batch_stats st;
   double t0 = now_s();
-  int rc = bc_gpu_mul_batch(d, n, &st);
+  int rc = bc_gpu_mul_batch_flags(d, n, BC_BATCH_HOST_OPERANDS, &st);
   count(n, 1, now_s() - t0);
+  __atomic_add_fetch(&g_device_us, (unsigned long long)(st.device_ms * 1000.0), __ATOMIC_RELAXED);
   free(d);
   if (rc != BC_OK) {
     fprintf(stderr, "bigfloat_mul_batch: GPU batch of %zu products failed: %s\n", n, bc_gpu_strerror(rc));
@@ -193,11 +195,13 @@ void _karatzuba_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *
 void bigfloat_get_counters(bigfloat_mul_counters *out) {
   pthread_mutex_lock(&g_cnt_mu);
   *out = g_cnt;
+  out->gpu_kernel_seconds = 1e-6 * (double)__atomic_load_n(&g_device_us, __ATOMIC_RELAXED);
   pthread_mutex_unlock(&g_cnt_mu);
 }
 
 void bigfloat_reset_counters(void) {
   pthread_mutex_lock(&g_cnt_mu);
   memset(&g_cnt, 0, sizeof g_cnt);
+  __atomic_store_n(&g_device_us, 0, __ATOMIC_RELAXED);
   pthread_mutex_unlock(&g_cnt_mu);
 }

@@ -98,6 +98,12 @@ int bc_gpu_mul(uint32_t *C, size_t CL, const uint32_t *A, size_t AL,
  * bucketed by transform length and every pass covers a whole bucket. */
 int bc_gpu_mul_batch(const bc_mul_desc *items, size_t n, bc_batch_stats *stats);
 
+/* Same, with hints: BC_BATCH_HOST_OPERANDS declares every A, B and C to be
+ * host memory (skips the per-pointer device query, which dominates batches
+ * of millions of small products). */
+enum { BC_BATCH_HOST_OPERANDS = 1 };
+int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, bc_batch_stats *stats);
+
 /* Launch on this CUDA stream (cudaStream_t as void*; NULL = library stream).
  * Calls still return only when their results are complete. */
 int bc_gpu_set_stream(void *stream);

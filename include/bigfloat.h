@@ -80,7 +80,8 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir);
 /* Product counters since the last reset (for tests and benchmarks). */
 typedef struct {
   size_t gpu_products, gpu_calls, small_products;
-  double gpu_seconds;
+  double gpu_seconds;         /* wall time inside GPU calls (batch calls only for kernels) */
+  double gpu_kernel_seconds;  /* GPU kernel time of the batch calls */
 } bigfloat_mul_counters;
 void bigfloat_get_counters(bigfloat_mul_counters *out);
 void bigfloat_reset_counters(void);

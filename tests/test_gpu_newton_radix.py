@@ -1,0 +1,103 @@
+"""GPU: Newton reciprocal and division and radix conversion of random
+bigfloats through the host library (products on the GPU), against the
+reference's own results (tests/golden/newton_radix.json, generated by
+tests/golden/make_newton_radix.py from the reference's bigfloat/rcp.c,
+div.c, radix.c and string.c), plus a 50-million-digit case beyond the
+reference's reach checked by modular verification of every product and by
+x * rcp(x) = 1 - eps."""
+import hashlib
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+from make_newton_radix import decimal_digits, operands, record  # noqa: E402
+
+GOLD = json.load(open(os.path.join(ROOT, "tests", "golden", "newton_radix.json")))["cases"]
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib():
+    from bluecrunch_b200.bigfloat import Lib
+    return Lib()
+
+
+@pytest.mark.parametrize("case", GOLD, ids=lambda c: "n%d" % c["n"])
+@pytest.mark.parametrize("driver", ["levels", "percall"])
+def test_matches_reference(case, driver, monkeypatch):
+    if driver == "percall":
+        if case["n"] > 110_000:
+            pytest.skip("per-call driver checked on the smaller cases")
+        monkeypatch.setenv("BC_RADIX_PERCALL", "1")
+    else:
+        monkeypatch.delenv("BC_RADIX_PERCALL", raising=False)
+    lib = _lib()
+    n = case["n"]
+    xl, yl = operands(case["seed"], n)
+    x = lib.make(xl, exp=-(n - 1))
+    y = lib.make(yl, exp=-(n - 1))
+    r, q, d = lib.make(), lib.make(), lib.make()
+    lib.rcp(r, x, n)
+    assert record(r) == case["rcp"]
+    lib.div(q, y, x, n)
+    assert record(q) == case["div"]
+    lib.radix(d, x)
+    assert record(d) == case["radix"]
+    s = lib.string(d, decimal_digits(n), 10)
+    assert s[:24].decode() == case["string_head"]
+    assert hashlib.sha256(s).hexdigest() == case["string_sha256"]
+    for z in (x, y, r, q, d):
+        lib.free(z)
+
+
+_BIG = r"""
+import sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {golden!r})
+from bluecrunch_b200.bigfloat import Lib, value
+from make_newton_radix import operands, decimal_digits
+n = {n}
+lib = Lib()
+xl, yl = operands(7, n)
+x = lib.make(xl, exp=-(n - 1)); r = lib.make(); m = lib.make(); d = lib.make()
+lib.rcp(r, x, n)
+lib.mul(m, x, r, 0)
+s, e, v = value(m)
+one = 1 << (-32 * e)
+err = abs(v - one)
+assert s == 1 and err * (1 << (32 * (n - 2))) <= one, "x*rcp(x) too far from 1"
+lib.radix(d, x)
+out = lib.string(d, decimal_digits(n), 10)
+bad = [i for i in range(2, min(len(out), 10**6)) if not 48 <= out[i] <= 57][:5]
+info = "len %d want %d, d.len %d d.exp %d, head %r, tail %r, non-digits at %r" % (
+    len(out), decimal_digits(n) - 1, d.len, d.exp, out[:30], out[-30:], bad)
+# a truncated output is "2." and digits - 3 digits (bigfloat/string.c:117-121)
+assert out.startswith(b"2.") and len(out) == decimal_digits(n) - 1 and out[2:].isdigit(), info
+# the first 10,000 digits from x's top 1,200 limbs, exactly (the dropped limbs
+# are below 10^-11000)
+sys.set_int_max_str_digits(0)
+top = 1200
+xv = int.from_bytes(xl[-top:].astype("<u4").tobytes(), "little")
+want = str(xv * 10**10000 >> (32 * (top - 1)))
+assert out[:10002] == (want[0] + "." + want[1:]).encode(), "leading digits differ"
+print("OK", r.len, d.len)
+"""
+
+
+def test_fifty_million_digits_verified():
+    """C4: a random 50,000,000-digit bigfloat (5,190,471 limbs): reciprocal at
+    full precision and conversion to decimal, every GPU product checked
+    modulo primes (BC_VERIFY=1 aborts on a mismatch)."""
+    n = 5_190_471
+    code = _BIG.format(root=ROOT, golden=os.path.join(ROOT, "tests", "golden"), n=n)
+    env = dict(os.environ, BC_VERIFY="1")
+    env.pop("BC_RADIX_PERCALL", None)
+    p = subprocess.run([sys.executable, "-c", code], env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                       text=True, timeout=900)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.strip().splitlines()[-1].startswith("OK"), p.stdout[-2000:]
