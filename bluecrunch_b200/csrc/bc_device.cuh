@@ -106,6 +106,23 @@ __device__ __forceinline__ void dftR(double2 *x) {
 
 constexpr int PTS = 8;
 
+// Barrier policies for block_fft: the threads that exchange data through
+// shared memory in one transform.  CtaSync: the whole CTA.  GroupSync<N>:
+// the N threads (N a multiple of 32) of group g, on named barrier 1 + g;
+// N == 32 is a single warp (__syncwarp).  Groups must not share shared
+// memory while a transform runs.
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+template <int N> struct GroupSync {
+  static_assert(N % 32 == 0, "named barriers count whole warps");
+  int id;
+  __device__ __forceinline__ void operator()() const {
+    if constexpr (N == 32) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(N) : "memory");
+  }
+};
+
 constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x / 2); }
 
 template <int L> struct Radices {
@@ -129,7 +146,9 @@ template <int L, int W> struct TileSmem {
 
 // One register stage of radix R at span NS (Stockham, twiddle before the
 // butterfly: x_r *= w^{(j mod NS) r}, w = e^{-+2 pi i/(NS R)}).  tw[m] holds
-// e^{-2 pi i m/L}.  Outputs stay in registers at v[q + r*(8/R)], whose
+// e^{-2 pi i m/L} (global or shared memory); the largest m any stage reads
+// is below 3L/4 (radix 8 reads r*k*L/(8 NS) for r <= 4, radix 4 up to
+// 3*k*L/(4 NS), radix 2 k*L/(2 NS), k < NS), so tw_entries<L>() entries suffice.  Outputs stay in registers at v[q + r*(8/R)], whose
 // destination row is (j/NS)*NS*R + j%NS + r*NS.
 template <int L, int R, int NS, bool INV>
 __device__ __forceinline__ void reg_stage(double2 (&v)[PTS], int t, const double2 *__restrict__ tw) {
@@ -145,14 +164,14 @@ __device__ __forceinline__ void reg_stage(double2 (&v)[PTS], int t, const double
       constexpr int step = L / (NS * R);
       if constexpr (R == 8) {
         // w^1, w^2, w^4 from the table, the other powers by one product each
-        const double2 w1 = __ldg(&tw[k * step]), w2 = __ldg(&tw[2 * k * step]), w4 = __ldg(&tw[4 * k * step]);
+        const double2 w1 = tw[k * step], w2 = tw[2 * k * step], w4 = tw[4 * k * step];
         const double2 w3 = cmul(w1, w2), w5 = cmul(w1, w4), w6 = cmul(w2, w4), w7 = cmul(w3, w4);
         x[1] = ctw<INV>(x[1], w1); x[2] = ctw<INV>(x[2], w2); x[3] = ctw<INV>(x[3], w3);
         x[4] = ctw<INV>(x[4], w4); x[5] = ctw<INV>(x[5], w5); x[6] = ctw<INV>(x[6], w6);
         x[7] = ctw<INV>(x[7], w7);
       } else {
 #pragma unroll
-        for (int r = 1; r < R; r++) x[r] = ctw<INV>(x[r], __ldg(&tw[k * r * step]));
+        for (int r = 1; r < R; r++) x[r] = ctw<INV>(x[r], tw[k * r * step]);
       }
     }
     dftR<R, INV>(x);
@@ -160,6 +179,8 @@ __device__ __forceinline__ void reg_stage(double2 (&v)[PTS], int t, const double
     for (int r = 0; r < R; r++) v[q + r * Q] = x[r];
   }
 }
+
+template <int L> __host__ __device__ constexpr int tw_entries() { return (3 * L) / 4; }
 
 template <int L, int R, int NS, int W>
 __device__ __forceinline__ void reg_stage_store(const double2 (&v)[PTS], int t, int s, double2 *sm) {
@@ -189,8 +210,8 @@ __device__ __forceinline__ void store_regs(const double2 (&v)[PTS], int t, int s
 
 // Radix-3 first stage (NS = 1, no twiddles) run from shared memory: the L/3
 // butterflies of each column are spread over the column's L/8 threads.
-template <int L, int W, bool INV>
-__device__ __forceinline__ void smem_radix3_stage(int t, int s, double2 *sm) {
+template <int L, int W, bool INV, class Sync>
+__device__ __forceinline__ void smem_radix3_stage(int t, int s, double2 *sm, const Sync &sync) {
   constexpr int TC = L / PTS, NB = L / 3;
   constexpr int MAXB = (NB + TC - 1) / TC;
   double2 a[MAXB][3];
@@ -203,7 +224,7 @@ __device__ __forceinline__ void smem_radix3_stage(int t, int s, double2 *sm) {
       dft3<INV>(a[q][0], a[q][1], a[q][2]);
     }
   }
-  __syncthreads();
+  sync();
 #pragma unroll
   for (int q = 0; q < MAXB; q++) {
     const int j = t + q * TC;
@@ -212,23 +233,23 @@ __device__ __forceinline__ void smem_radix3_stage(int t, int s, double2 *sm) {
       for (int r = 0; r < 3; r++) sm[sidx<L, W>(3 * j + r, s)] = a[q][r];
     }
   }
-  __syncthreads();
+  sync();
 }
 
 // Radix-8 stages k..n8-1, then the remainder stage; NS is the span so far.
-template <int L, int W, bool INV, int NS, int K>
+template <int L, int W, bool INV, int NS, int K, class Sync>
 __device__ __forceinline__ void run_pow2_stages(double2 (&v)[PTS], int t, int s, double2 *sm,
-                                                const double2 *__restrict__ tw) {
+                                                const double2 *__restrict__ tw, const Sync &sync) {
   using RX = Radices<L>;
   if constexpr (K < RX::n8) {
     reg_stage<L, 8, NS, INV>(v, t, tw);
     constexpr bool last = (K + 1 == RX::n8) && (RX::rem == 1);
     if constexpr (!last) {
       reg_stage_store<L, 8, NS, W>(v, t, s, sm);
-      __syncthreads();
+      sync();
       load_regs<L, W>(v, t, s, sm);
-      __syncthreads();
-      run_pow2_stages<L, W, INV, NS * 8, K + 1>(v, t, s, sm, tw);
+      sync();
+      run_pow2_stages<L, W, INV, NS * 8, K + 1>(v, t, s, sm, tw, sync);
     }
   } else if constexpr (RX::rem > 1) {
     reg_stage<L, RX::rem, NS, INV>(v, t, tw);
@@ -236,22 +257,22 @@ __device__ __forceinline__ void run_pow2_stages(double2 (&v)[PTS], int t, int s,
 }
 
 // Full block FFT.  v in/out per the register contract; sm is this tile's
-// shared memory; tw = e^{-2 pi i m/L}, m < L.  Ends with all threads past a
-// barrier so sm may be reused.
-template <int L, int W, bool INV>
+// shared memory; tw = e^{-2 pi i m/L}, m < tw_entries<L>().  Ends with the
+// threads of the sync group past a barrier, so the group may reuse sm.
+template <int L, int W, bool INV, class Sync = CtaSync>
 __device__ __forceinline__ void block_fft(double2 (&v)[PTS], int t, int s, double2 *sm,
-                                          const double2 *__restrict__ tw) {
+                                          const double2 *__restrict__ tw, const Sync &sync = Sync{}) {
   using RX = Radices<L>;
   static_assert(L % PTS == 0, "block length must be a multiple of 8");
   if constexpr (RX::has3) {
     store_regs<L, W>(v, t, s, sm);
-    __syncthreads();
-    smem_radix3_stage<L, W, INV>(t, s, sm);
+    sync();
+    smem_radix3_stage<L, W, INV>(t, s, sm, sync);
     load_regs<L, W>(v, t, s, sm);
-    __syncthreads();
-    run_pow2_stages<L, W, INV, 3, 0>(v, t, s, sm, tw);
+    sync();
+    run_pow2_stages<L, W, INV, 3, 0>(v, t, s, sm, tw, sync);
   } else {
-    run_pow2_stages<L, W, INV, 1, 0>(v, t, s, sm, tw);
+    run_pow2_stages<L, W, INV, 1, 0>(v, t, s, sm, tw, sync);
   }
 }
 

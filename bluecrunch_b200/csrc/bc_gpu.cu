@@ -363,25 +363,24 @@ template <int L>
 KInfo outer_fwd_info() {
   using T = PassTile<L>;
   using K = PackTile<L>;
-  return {(const void *)k2_outer_fwd<L>, T::NT, (size_t)L * T::W * 16 + 2 * (size_t)K::STAGE_WORDS * 4 + 1024,
-          "outer_fwd", SIG_P};
+  return {(const void *)k2_outer_fwd<L>, T::NT, K::SMEM, "outer_fwd", SIG_P};
 }
 template <int L>
 KInfo outer_inv_info() {
   using T = PassTile<L>;
-  return {(const void *)k2_outer_inv<L>, T::NT, 2 * (size_t)L * T::W * 16 + 1024, "outer_inv", SIG_P_MAP,
+  return {(const void *)k2_outer_inv<L>, T::NT, T::SMEM_OUTER_INV, "outer_inv", SIG_P_MAP,
           T::BOX_ROWS, T::BYTES, T::HALVES};
 }
 template <int L, bool INV>
 KInfo mid_info() {
   using T = PassTile<L>;
-  return {(const void *)k2_mid<L, INV>, T::NT, 2 * (size_t)L * T::W * 16 + 1024, INV ? "mid_inv" : "mid_fwd",
+  return {(const void *)k2_mid<L, INV>, T::NT, T::SMEM_MID, INV ? "mid_inv" : "mid_fwd",
           SIG_P_MAP2, T::BOX_ROWS, T::BYTES, T::HALVES};
 }
 template <int L, bool SQ>
 KInfo rows_info() {
   using R = RowTile<L>;
-  return {(const void *)k2_rows<L, SQ>, R::NT, 3 * (size_t)R::NR * L * 16 + 1024, "rows", SIG_P_MAP2,
+  return {(const void *)k2_rows<L, SQ>, R::NT, R::SMEM, "rows", SIG_P_MAP2,
           R::BOX_LINES, (unsigned)(R::NR * L * 16), R::PARTS};
 }
 template <int M, bool SQ>

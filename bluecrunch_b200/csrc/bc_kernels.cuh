@@ -29,6 +29,7 @@
 #pragma once
 #include <cuda/atomic>
 
+#include "bc_async.cuh"
 #include "bc_device.cuh"
 
 namespace bc {
@@ -184,6 +185,8 @@ constexpr int LOOKBACK_SPINS = 1 << 22;
 
 __device__ __forceinline__ U192 rec_h(const RunRec &r) { U192 h = {{r.h0, r.h1, r.h2}}; return h; }
 
+// Words of run r (bits [r nbits, (r+1) nbits)) below nwords; a word that
+// straddles into run r+1 takes its high bits from hn.
 __device__ __forceinline__ void write_run_words(uint32_t *C, unsigned long long nwords, unsigned long long r,
                                                 int nbits, const U192 &h, const U192 &hn) {
   const unsigned long long bit0 = r * (unsigned long long)nbits;
@@ -197,16 +200,29 @@ __device__ __forceinline__ void write_run_words(uint32_t *C, unsigned long long 
   }
 }
 
+// 16-byte chunk c of a staged tile of run records lives at chunk position
+// (c & ~7) | ((c ^ (c >> 3)) & 7): the 8 chunks of one thread's 4 records
+// (8t .. 8t+7) land on 8 distinct bank groups across any 8 threads.
+__device__ __forceinline__ int rec_chunk_pos(int c) { return (c & ~7) | ((c ^ (c >> 3)) & 7); }
+
+// Corrected run values of a tile as three 64-bit planes (plane stride
+// CARRY_TILE_RUNS + 1 words: entry CARRY_TILE_RUNS is the run after the
+// tile's last one, for the word that straddles it).
+constexpr int HC_STRIDE = CARRY_TILE_RUNS + 1;
+
 __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
+  // records of the tile (32 KB), then reused for the corrected values
+  __shared__ __align__(16) unsigned long long srec[CARRY_TILE_RUNS * 4];
+  static_assert(3 * HC_STRIDE <= CARRY_TILE_RUNS * 4, "corrected values fit the record buffer");
   __shared__ uint32_t sw[65];
   __shared__ unsigned long long s_unit;
   __shared__ int s_delta;
+  __shared__ long long s_cprev;
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) s_unit = atomicAdd(p.counter, 1u);
     __syncthreads();
     const unsigned long long unit = s_unit;
-    __syncthreads();
     if (unit >= p.carry_tiles) break;
     // find the item owning this tile (items are ordered by tile0)
     int lo = 0, hi = p.nitems - 1;
@@ -216,32 +232,53 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
     }
     const ItemDesc &it = p.items[lo];
     const unsigned long long tile = unit - it.tile0;
-    // this thread's CARRY_RPT consecutive runs
-    const unsigned long long r0 = tile * CARRY_TILE_RUNS + (unsigned long long)tid * CARRY_RPT;
+    const unsigned long long rt = tile * CARRY_TILE_RUNS;  // first run of the tile
+    const unsigned long long nruns = it.nruns;
+    const int nr = (int)min((unsigned long long)CARRY_TILE_RUNS, nruns - rt);  // runs of this tile
     const int nbits = 8 * it.b;
     const unsigned long long nrec = (unsigned long long)(2 * p.M) / 8;
+    // ---- stage the tile's records (coalesced 16-byte copies) and C_{rt-1}
+    {
+      const char *src = reinterpret_cast<const char *>(it.rec + rt);
+      char *dst = reinterpret_cast<char *>(srec);
+      const int nch = 2 * nr;
+      for (int c = tid; c < 2 * CARRY_TILE_RUNS; c += CARRY_NT)
+        cp_async16(dst + 16 * rec_chunk_pos(c), src + (c < nch ? 16 * c : 0), c < nch ? 16 : 0);
+      cp_async_commit();
+      if (tid == 0) s_cprev = rt > 0 ? load_rec(&it.rec[rt - 1]).c : 0;
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    // ---- this thread's CARRY_RPT consecutive runs
+    const int k0 = tid * CARRY_RPT;
     U192 h[CARRY_RPT];
     long long c[CARRY_RPT];
     uint32_t f[CARRY_RPT];
     uint32_t F = FN_ID;
-    long long cprev = (r0 > 0 && r0 < it.nruns) ? load_rec(&it.rec[r0 - 1]).c : 0;
+    long long cprev = s_cprev;
+    if (k0 > 0 && k0 <= nr) {
+      const int ch = rec_chunk_pos(2 * (k0 - 1) + 1);  // second chunk of record k0-1: (h2, c)
+      cprev = (long long)srec[2 * ch + 1];
+    }
 #pragma unroll
     for (int q = 0; q < CARRY_RPT; q++) {
-      const unsigned long long r = r0 + q;
+      const int k = k0 + q;
       f[q] = FN_ID;
       c[q] = 0;
       h[q].w[0] = h[q].w[1] = h[q].w[2] = 0;
-      if (r < it.nruns) {
-        RunRec rr = load_rec(&it.rec[r]);
-        h[q] = rec_h(rr);
-        c[q] = rr.c;
+      if (k < nr) {
+        const int ca = rec_chunk_pos(2 * k), cb = rec_chunk_pos(2 * k + 1);
+        h[q].w[0] = srec[2 * ca];
+        h[q].w[1] = srec[2 * ca + 1];
+        h[q].w[2] = srec[2 * cb];
+        c[q] = (long long)srec[2 * cb + 1];
         f[q] = run_transfer(h[q], cprev, nbits);
-        cprev = rr.c;
+        cprev = c[q];
         F = fn_compose(F, f[q]);
       }
     }
     uint32_t agg;
-    const uint32_t ex = block_scan_fn<CARRY_NT>(F, sw, &agg);
+    const uint32_t ex = block_scan_fn<CARRY_NT>(F, sw, &agg);  // ends past a barrier: srec is free
     if (tid == 0) {
       // A tile whose composed map is constant knows its carry out before its
       // carry in: it publishes that at once, and a lookback that meets such an
@@ -283,32 +320,55 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
       s_delta = din;
     }
     __syncthreads();
-    // carries into each run, then the words
-    int d = fn_apply(ex, s_delta);  // delta into run r0
-    int dout[CARRY_RPT];
+    // ---- carries into each run; corrected values to shared memory
+    unsigned long long *hc = srec;
+    int d = fn_apply(ex, s_delta);  // delta into run k0
 #pragma unroll
     for (int q = 0; q < CARRY_RPT; q++) {
-      if (r0 + q < it.nruns) {
+      const int k = k0 + q;
+      if (k < nr) {
         u192_add_delta(h[q], d, nbits);
         d = fn_apply(f[q], d);
+        hc[k] = h[q].w[0];
+        hc[HC_STRIDE + k] = h[q].w[1];
+        hc[2 * HC_STRIDE + k] = h[q].w[2];
+        if (k + 1 == nr) {
+          // the run after the tile's last one, for a word that straddles it:
+          // inside this item only when the item ends inside this tile
+          U192 hn = {{0, 0, 0}};
+          const unsigned long long r = rt + k;
+          if (nr < CARRY_TILE_RUNS && r + 1 < nrec) {
+            RunRec rn = load_rec(&it.rec[r + 1]);
+            hn = rec_h(rn);
+            (void)u192_add_s64(hn, c[q], nbits);
+            u192_add_delta(hn, d, nbits);
+          }
+          hc[nr] = hn.w[0];
+          hc[HC_STRIDE + nr] = hn.w[1];
+          hc[2 * HC_STRIDE + nr] = hn.w[2];
+          if (r + 1 == nrec && c[q] + d != 0) atomicOr(it.flags, FLAG_TOPCARRY);
+        }
       }
-      dout[q] = d;
     }
-#pragma unroll
-    for (int q = 0; q < CARRY_RPT; q++) {
-      const unsigned long long r = r0 + q;
-      if (r >= it.nruns) break;
-      U192 hn = {{0, 0, 0}};
-      if (q + 1 < CARRY_RPT && r + 1 < it.nruns) {
-        hn = h[q + 1];
-      } else if (r + 1 < nrec) {
-        RunRec rn = load_rec(&it.rec[r + 1]);
-        hn = rec_h(rn);
-        (void)u192_add_s64(hn, c[q], nbits);
-        u192_add_delta(hn, dout[q], nbits);
+    __syncthreads();
+    // ---- words of the tile, one per thread per step (coalesced stores).
+    // The tile starts on a word boundary (1024 runs of 8b bits).
+    {
+      const unsigned long long w0 = rt * (unsigned long long)nbits / 32;
+      const unsigned long long wend =
+          min(it.nwords, (rt * (unsigned long long)nbits + (unsigned long long)nr * nbits + 31) / 32);
+      const int nw = wend > w0 ? (int)(wend - w0) : 0;
+      for (int i = tid; i < nw; i += CARRY_NT) {
+        const int bit = 32 * i;
+        const int k = bit / nbits, off = bit - k * nbits;
+        U192 hk = {{hc[k], hc[HC_STRIDE + k], hc[2 * HC_STRIDE + k]}};
+        uint32_t x = u192_bits32(hk, off);
+        if (off + 32 > nbits) {
+          U192 hn = {{hc[k + 1], hc[HC_STRIDE + k + 1], hc[2 * HC_STRIDE + k + 1]}};
+          x |= u192_bits32(hn, 0) << (nbits - off);
+        }
+        it.C[w0 + i] = x;
       }
-      write_run_words(it.C, it.nwords, r, nbits, h[q], hn);
-      if (r + 1 == nrec && c[q] + dout[q] != 0) atomicOr(it.flags, FLAG_TOPCARRY);
     }
     // zero any words beyond the product (CL > product length)
     if (tile == 0) {

@@ -10,6 +10,8 @@
 // All items of a class sit in contiguous slabs (item i's buffer at i*M), so
 // one tensor map per slab serves the whole class.
 #pragma once
+#include <type_traits>
+
 #include "bc_async.cuh"
 #include "bc_kernels.cuh"
 
@@ -23,7 +25,19 @@ template <int L> struct PassTile {
   static constexpr int HALVES = L / BOX_ROWS;
   static constexpr unsigned BYTES = (unsigned)L * W * 16;
   static constexpr int MINB = NT <= 256 ? 2 : 1;  // resident CTAs per SM the register budget allows for
+  static constexpr int TWN = tw_entries<L>();     // L-point stage twiddles kept in shared memory
+  // dynamic shared memory of k2_mid / k2_outer_inv: two tiles, the stage
+  // twiddles, the outer pass's weights (outer_inv only), 1024 bytes of slack
+  // for aligning the tiles
+  static constexpr size_t SMEM_MID = 2 * (size_t)BYTES + (size_t)TWN * 16 + 1024;
+  static constexpr size_t SMEM_OUTER_INV = SMEM_MID + (size_t)L * 16;
 };
+
+// Copy n table entries from global to shared memory (all threads of the CTA;
+// the caller's next barrier publishes them).
+__device__ __forceinline__ void table_to_smem(double2 *dst, const double2 *__restrict__ src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(&src[i]);
+}
 
 __device__ __forceinline__ double2 *align1024(unsigned char *p) {
   return reinterpret_cast<double2 *>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
@@ -83,27 +97,28 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
   constexpr int W = T::W, TC = L / PTS;
   extern __shared__ unsigned char smraw[];
   __shared__ uint64_t bars[2];
-  double2 *buf[2];
-  buf[0] = align1024(smraw);
-  buf[1] = buf[0] + L * W;
+  double2 *const buf0 = align1024(smraw);  // stage st's tile at buf0 + st * L * W
+  double2 *twS = buf0 + 2 * L * W;
+  table_to_smem(twS, p.twL2, T::TWN);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
-  const int tiles = p.Lr / W;
-  const int nops = (INV || p.sq) ? 1 : 2;
-  const long long per_op = (long long)p.L1 * tiles, per_item = nops * per_op;
-  const long long total = (long long)p.nitems * per_item;
-  auto decode = [&](long long u, int &item, int &op, int &blk, int &tile) {
+  // unit counts stay far below 2^32 (a class holds at most 2^33 points, 2048 per unit)
+  const unsigned tiles = p.Lr / W;
+  const unsigned nops = (INV || p.sq) ? 1 : 2;
+  const unsigned per_op = (unsigned)p.L1 * tiles, per_item = nops * per_op;
+  const unsigned total = (unsigned)p.nitems * per_item;
+  auto decode = [&](unsigned u, int &item, int &op, int &blk, int &tile) {
     item = (int)(u / per_item);
-    long long r = u % per_item;
+    unsigned r = u - (unsigned)item * per_item;
     op = (int)(r / per_op);
-    r %= per_op;
+    r -= (unsigned)op * per_op;
     blk = (int)(r / tiles);
-    tile = (int)(r % tiles);
+    tile = (int)(r - (unsigned)blk * tiles);
   };
-  auto issue = [&](long long u, int st) {
+  auto issue = [&](unsigned u, int st) {
     int item, op, blk, tile;
     decode(u, item, op, blk, tile);
     fence_proxy_async_smem();
-    tile_load_4d<L, W>(buf[st], op ? &mB : &mA, &bars[st], tile * W, blk, item);
+    tile_load_4d<L, W>(buf0 + st * L * W, op ? &mB : &mA, &bars[st], tile * W, blk, item);
   };
   if (tid == 0) {
     mbar_init(&bars[0], 1);
@@ -111,36 +126,37 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
     fence_mbar_init();
   }
   __syncthreads();
-  unsigned phase[2] = {0u, 0u};
+  unsigned phases = 0;  // bit st: parity to wait for on bars[st]
   int st = 0;
-  long long u = blockIdx.x;
+  unsigned u = blockIdx.x;
   if (tid == 0 && u < total) issue(u, 0);
   for (; u < total; u += gridDim.x) {
-    const long long un = u + gridDim.x;
+    const unsigned un = u + gridDim.x;
     if (tid == 0 && un < total) issue(un, st ^ 1);
     int item, op, blk, tile;
     decode(u, item, op, blk, tile);
     const ItemDesc &it = p.items[item];
-    const bool ok = mbar_wait(&bars[st], phase[st]);
-    phase[st] ^= 1;
-    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
-    double2 *bf = buf[st];
-    double2 *g = (op ? it.bufB : it.bufA) + (uint64_t)blk * p.S1;
+    double2 *g = (op ? it.bufB : it.bufA) + (unsigned)blk * (unsigned)p.S1;
     const int col = tile * W + s;
     double2 v[PTS], w[PTS];
     // e^{-2 pi i col k2/(L2 Lr)} = table index 4 L1 col k2 of the 4M table
+    // (global loads issued before the wait so their latency overlaps it)
     twiddle_run(p.tw4M, (uint64_t)4 * p.L1 * col * t, false, (uint64_t)4 * p.L1 * col * TC, w);
+    const bool ok = mbar_wait(&bars[st], (phases >> st) & 1u);
+    phases ^= 1u << st;
+    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+    double2 *bf = buf0 + st * L * W;
 #pragma unroll
     for (int i = 0; i < PTS; i++) {
       v[i] = bf[bidx<L>(t + i * TC, s)];
       if (INV) v[i] = cmulc(v[i], w[i]);
     }
     __syncthreads();
-    block_fft<L, W, INV>(v, t, s, bf, p.twL2);
+    block_fft<L, W, INV>(v, t, s, bf, twS);
 #pragma unroll
     for (int i = 0; i < PTS; i++) {
-      const int k2 = t + i * TC;
-      g[(uint64_t)k2 * p.Lr + col] = INV ? v[i] : cmul(v[i], w[i]);
+      const unsigned k2 = t + i * TC;
+      g[k2 * (unsigned)p.Lr + col] = INV ? v[i] : cmul(v[i], w[i]);
     }
     __syncthreads();
     st ^= 1;
@@ -155,49 +171,51 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_i
   constexpr int W = T::W, TC = L / PTS, G = W / 8;
   extern __shared__ unsigned char smraw[];
   __shared__ uint64_t bars[2];
-  double2 *buf[2];
-  buf[0] = align1024(smraw);
-  buf[1] = buf[0] + L * W;
+  double2 *const buf0 = align1024(smraw);  // stage st's tile at buf0 + st * L * W
+  double2 *twS = buf0 + 2 * L * W;
+  double2 *pwS = twS + T::TWN;
+  table_to_smem(twS, p.twL1, T::TWN);
+  table_to_smem(pwS, p.pw_inv, L);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
-  const int tiles = p.S1 / W;
-  const long long total = (long long)p.nitems * tiles;
+  const unsigned tiles = p.S1 / W;
+  const unsigned total = (unsigned)p.nitems * tiles;  // far below 2^32
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  unsigned phase[2] = {0u, 0u};
+  unsigned phases = 0;  // bit st: parity to wait for on bars[st]
   int st = 0;
-  long long u = blockIdx.x;
+  unsigned u = blockIdx.x;
   if (tid == 0 && u < total) {
     fence_proxy_async_smem();
-    tile_load_3d<L, W>(buf[0], &mA, &bars[0], (int)(u % tiles) * W, (int)(u / tiles));
+    tile_load_3d<L, W>(buf0, &mA, &bars[0], (int)(u % tiles) * W, (int)(u / tiles));
   }
   for (; u < total; u += gridDim.x) {
-    const long long un = u + gridDim.x;
+    const unsigned un = u + gridDim.x;
     if (tid == 0 && un < total) {
       fence_proxy_async_smem();
-      tile_load_3d<L, W>(buf[st ^ 1], &mA, &bars[st ^ 1], (int)(un % tiles) * W, (int)(un / tiles));
+      tile_load_3d<L, W>(buf0 + (st ^ 1) * L * W, &mA, &bars[st ^ 1], (int)(un % tiles) * W, (int)(un / tiles));
     }
     const int item = (int)(u / tiles), tile = (int)(u % tiles);
     const ItemDesc &it = p.items[item];
-    const bool ok = mbar_wait(&bars[st], phase[st]);
-    phase[st] ^= 1;
-    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
-    double2 *bf = buf[st];
     const int col = tile * W + s;
     double2 v[PTS], w[PTS];
-    outer_twiddles<TC>(p.tw4M, col, t, w);
+    outer_twiddles<TC>(p.tw4M, col, t, w);  // global loads, before the wait
+    const bool ok = mbar_wait(&bars[st], (phases >> st) & 1u);
+    phases ^= 1u << st;
+    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+    double2 *bf = buf0 + st * L * W;
 #pragma unroll
     for (int i = 0; i < PTS; i++) v[i] = cmulc(bf[bidx<L>(t + i * TC, s)], w[i]);
     __syncthreads();
-    block_fft<L, W, true>(v, t, s, bf, p.twL1);
+    block_fft<L, W, true>(v, t, s, bf, twS);
     double err = 0.0;
 #pragma unroll
     for (int i = 0; i < PTS; i++) {
       const int n1 = t + i * TC;
-      double2 z = cmul(v[i], __ldg(&p.pw_inv[n1]));
+      double2 z = cmul(v[i], pwS[n1]);
       double re = rint(z.x), im = rint(z.y);
       err = fmax(err, round_check(z, re, im));
       bf[bidx<L>(n1, s)] = make_double2(re, im);
@@ -215,7 +233,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_i
         cre[q] = z.x;
         cim[q] = z.y;
       }
-      const uint64_t n0 = (uint64_t)row * p.S1 + (uint64_t)tile * W + 8 * gi;
+      const unsigned n0 = (unsigned)row * (unsigned)p.S1 + (unsigned)tile * W + 8 * gi;
       store_rec(&it.rec[n0 >> 3], make_run(cre, it.b));
       store_rec(&it.rec[(n0 + p.M) >> 3], make_run(cim, it.b));
     }
@@ -244,10 +262,26 @@ template <int L> struct RowTile {
   static_assert(BOX_LINES * PARTS == LINES && BOX_LINES % 8 == 0, "row split into whole swizzle atoms");
   static_assert(PARTS == 1 || NR == 1, "split rows come one per unit");
   static constexpr int MINB = NT <= 256 ? 2 : 1;
+  // stage twiddles in shared memory where two CTAs per SM still fit
+  static constexpr bool TWS = L <= 1536;
+  static constexpr int TWN = TWS ? tw_entries<L>() : 0;
+  static constexpr size_t SMEM = 3 * (size_t)NR * L * 16 + (size_t)TWN * 16 + 1024;
+};
+
+// Barrier of one row's L/8 threads inside k2_rows: a named barrier when the
+// row is whole warps, the warp when a warp holds whole rows, else the CTA.
+template <int L> struct RowSyncOf {
+  static constexpr int TC = L / PTS;
+  using type = typename std::conditional<(TC % 32 == 0), GroupSync<TC>,
+                                         typename std::conditional<(32 % TC == 0), GroupSync<32>, CtaSync>::type>::type;
+  __device__ static type make(int row) {
+    if constexpr (std::is_same<type, CtaSync>::value) return CtaSync{};
+    else return type{1 + row};
+  }
 };
 
 template <int L>
-__device__ __forceinline__ void rows_load(double2 *dst, const CUtensorMap *map, uint64_t *bar, long long row0) {
+__device__ __forceinline__ void rows_load(double2 *dst, const CUtensorMap *map, uint64_t *bar, unsigned row0) {
   using R = RowTile<L>;
   mbar_expect_tx(bar, (unsigned)R::NR * L * 16);
   if (R::PARTS == 1) {
@@ -268,9 +302,15 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
   double2 *bufA = align1024(smraw);
   double2 *bufB = bufA + NR * L;
   double2 *bufS = bufB + NR * L;  // A's spectrum while B is transformed
+  const double2 *tw = p.twLr;
+  if constexpr (R::TWS) {
+    double2 *twS = bufS + NR * L;
+    table_to_smem(twS, p.twLr, R::TWN);
+    tw = twS;
+  }
   const int tid = threadIdx.x, rl = tid / TC, t = tid % TC;
-  const long long rows_item = p.M / L;
-  const long long total = (long long)p.nitems * rows_item / NR;
+  const unsigned rows_item = p.M / L;
+  const unsigned total = (unsigned)p.nitems * rows_item / NR;  // far below 2^32
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -278,26 +318,28 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
   }
   __syncthreads();
   unsigned phA = 0, phB = 0;
-  long long u = blockIdx.x;
+  unsigned u = blockIdx.x;
   if (tid == 0 && u < total) {
     fence_proxy_async_smem();
     rows_load<L>(bufA, &mA, &bars[0], u * NR);
     if (!SQ) rows_load<L>(bufB, &mB, &bars[1], u * NR);
   }
   double2 *smA = bufA + rl * L, *smB = bufB + rl * L, *smS = bufS + rl * L;
+  const auto rsync = RowSyncOf<L>::make(rl);  // the threads of this row
   for (; u < total; u += gridDim.x) {
-    const long long un = u + gridDim.x;
-    const long long grow = u * NR + rl;  // this thread's row in the class slab
-    const ItemDesc &it = p.items[grow / rows_item];
-    double2 *ra = it.bufA + (uint64_t)(grow % rows_item) * L;
+    const unsigned un = u + gridDim.x;
+    const unsigned grow = u * NR + rl;  // this thread's row in the class slab
+    const unsigned item = grow / rows_item;
+    const ItemDesc &it = p.items[item];
+    double2 *ra = it.bufA + (grow - item * rows_item) * (unsigned)L;
     double2 v[PTS];
     bool ok = mbar_wait(&bars[0], phA);
     phA ^= 1;
     if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
 #pragma unroll
     for (int i = 0; i < PTS; i++) v[i] = smA[ridx(t + i * TC)];
-    __syncthreads();
-    block_fft<L, 1, false>(v, t, 0, smA, p.twLr);
+    rsync();
+    block_fft<L, 1, false>(v, t, 0, smA, tw, rsync);
     if (SQ) {
 #pragma unroll
       for (int i = 0; i < PTS; i++) v[i] = cmul(v[i], v[i]);
@@ -316,19 +358,20 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
       if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
 #pragma unroll
       for (int i = 0; i < PTS; i++) v[i] = smB[ridx(t + i * TC)];
-      __syncthreads();
-      block_fft<L, 1, false>(v, t, 0, smB, p.twLr);
+      rsync();
+      block_fft<L, 1, false>(v, t, 0, smB, tw, rsync);
 #pragma unroll
       for (int i = 0; i < PTS; i++) v[i] = cmul(smS[ridx(t + i * TC)], v[i]);
+      __syncthreads();  // every row is done with B's buffer and with its spectrum reads
+      if (tid == 0 && un < total) {  // fetch the next rows of B during the inverse
+        fence_proxy_async_smem();
+        rows_load<L>(bufB, &mB, &bars[1], un * NR);
+      }
     }
-    block_fft<L, 1, true>(v, t, 0, SQ ? smS : smB, p.twLr);
+    // the inverse exchanges through the spectrum buffer, private to the row
+    block_fft<L, 1, true>(v, t, 0, smS, tw, rsync);
 #pragma unroll
     for (int i = 0; i < PTS; i++) ra[t + i * TC] = v[i];
-    __syncthreads();
-    if (!SQ && tid == 0 && un < total) {  // B's buffer is free after the inverse
-      fence_proxy_async_smem();
-      rows_load<L>(bufB, &mB, &bars[1], un * NR);
-    }
   }
 }
 
@@ -345,6 +388,9 @@ template <int L> struct PackTile {
   // staged segment: up to 3 extra words in front so 16-byte chunks align
   static constexpr int SEGW4 = (SEGW + 3 + 3) / 4 * 4;
   static constexpr int STAGE_WORDS = 2 * L * SEGW4;
+  // dynamic shared memory: tile, two limb stages, stage twiddles, weights, slack
+  static constexpr size_t SMEM = (size_t)L * W * 16 + 2 * (size_t)STAGE_WORDS * 4 + (size_t)tw_entries<L>() * 16 +
+                                 (size_t)L * 16 + 1024;
   // the 64-bit window of the last digit (b <= 24, shift <= 3 words) stays inside
   static_assert(SEGW4 >= ((158 + 24 * (W - 1)) >> 5) + 2, "staged segment too short");
 };
@@ -357,11 +403,15 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
   extern __shared__ unsigned char smraw[];
   double2 *tile = align1024(smraw);
   uint32_t *stg = reinterpret_cast<uint32_t *>(tile + L * W);  // 2 stages of STAGE_WORDS
+  double2 *twS = reinterpret_cast<double2 *>(stg + 2 * K::STAGE_WORDS);
+  double2 *pwS = twS + tw_entries<L>();
+  table_to_smem(twS, p.twL1, tw_entries<L>());
+  table_to_smem(pwS, p.pw_fwd, L);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   const int tiles = p.S1 / W;
   const int nops = p.sq ? 1 : 2;
-  const long long per_item = (long long)nops * tiles;
-  const long long total = (long long)p.nitems * per_item;
+  const unsigned per_item = (unsigned)(nops * tiles);
+  const unsigned total = (unsigned)p.nitems * per_item;  // far below 2^32
   // Row segment (n1, part) of tile tl starts one word below the word of digit
   // j0 = n1*S1 + tl*W + part*M.  S1 and M are multiples of 128, so that word is
   // n1*(S1 b/32) + part*(M b/32) + (tl*W*b >> 5), with the first two terms
@@ -371,44 +421,45 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
   auto seg_shift = [&](int tl, int b, bool al16) -> int {
     return al16 ? (int)((((long long)tl * W * b >> 5) - 1) & 3) : 0;
   };
-  auto stage_copy = [&](long long u, int st) {
+  auto stage_copy = [&](unsigned u, int st) {
     const int item = (int)(u / per_item), rem = (int)(u % per_item);
     const int op = rem / tiles, tl = rem % tiles;
     const ItemDesc &it = p.items[item];
     const uint32_t *X = op ? it.B : it.A;
-    const long long XL = (long long)(op ? it.BL : it.AL);
-    const long long b = it.b;
+    // word indices fit an int: operands and transforms stay below 2^29 words
+    const int XL = (int)(op ? it.BL : it.AL);
+    const int b = it.b;
     const bool al16 = op ? it.b16 : it.a16;
-    const long long RW = (long long)p.S1 * b / 32, PW = (long long)p.M * b / 32;
-    const long long wbase = (((long long)tl * W * b) >> 5) - 1 - seg_shift(tl, (int)b, al16);
+    const int RW = (int)((unsigned)p.S1 * (unsigned)b / 32), PW = (int)((unsigned)p.M * (unsigned)b / 32);
+    const int wbase = ((tl * W * b) >> 5) - 1 - seg_shift(tl, b, al16);
     uint32_t *dst = stg + st * K::STAGE_WORDS;
     if (al16) {
       constexpr int CH = K::SEGW4 / 4, NCH = 2 * L * CH;
       for (int idx = tid; idx < NCH; idx += NT) {
         const int segi = idx / CH, k = idx - segi * CH;
         const int part = segi >= L, row = segi - (part ? L : 0);
-        const long long w = row * RW + (part ? PW : 0) + wbase + 4 * k;  // multiple of 4
-        long long nv = XL - w;
+        const int w = row * RW + (part ? PW : 0) + wbase + 4 * k;  // multiple of 4
+        int nv = XL - w;
         nv = nv < 0 ? 0 : (nv > 4 ? 4 : nv);
         if (w < 0) nv = 0;
-        cp_async16(dst + segi * K::SEGW4 + 4 * k, X + (nv ? w : 0), (int)nv * 4);
+        cp_async16(dst + segi * K::SEGW4 + 4 * k, X + (nv ? w : 0), nv * 4);
       }
     } else {
       for (int idx = tid; idx < K::STAGE_WORDS; idx += NT) {
         const int segi = idx / K::SEGW4, k = idx - segi * K::SEGW4;
         const int part = segi >= L, row = segi - (part ? L : 0);
-        const long long w = row * RW + (part ? PW : 0) + wbase + k;
+        const int w = row * RW + (part ? PW : 0) + wbase + k;
         const bool in = w >= 0 && w < XL;
         cp_async4(dst + idx, X + (in ? w : 0), in ? 4 : 0);
       }
     }
   };
-  long long u = blockIdx.x;
+  unsigned u = blockIdx.x;
   int st = 0;
   if (u < total) stage_copy(u, 0);
   cp_async_commit();
   for (; u < total; u += gridDim.x) {
-    const long long un = u + gridDim.x;
+    const unsigned un = u + gridDim.x;
     if (un < total) stage_copy(un, st ^ 1);
     cp_async_commit();
     cp_async_wait<1>();
@@ -416,7 +467,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     const int item = (int)(u / per_item), rem = (int)(u % per_item);
     const int op = rem / tiles, tl = rem % tiles;
     const ItemDesc &it = p.items[item];
-    const unsigned long long nd = op ? it.ndB : it.ndA;
+    const unsigned nd = (unsigned)(op ? it.ndB : it.ndA);  // below 2^30
     double2 *gbuf = op ? it.bufB : it.bufA;
     const int b = it.b;
     const uint32_t *seg = stg + st * K::STAGE_WORDS;
@@ -425,7 +476,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     const unsigned rel = 32u * (1u + (unsigned)seg_shift(tl, b, al16)) + (unsigned)((tl * W * b) & 31) +
                          (unsigned)(s * b);  // bit of digit j0+s in its staged segment
     const unsigned wi = (rel - 1) >> 5, sh = (rel - 1) & 31;
-    const uint64_t mask = (1ull << b) - 1;
+    const unsigned mask = (1u << b) - 1;
     double2 v[PTS];
 #pragma unroll
     for (int i = 0; i < PTS; i++) {
@@ -433,20 +484,22 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
       double d[2];
 #pragma unroll
       for (int part = 0; part < 2; part++) {
-        const unsigned long long j = (unsigned long long)n1 * p.S1 + col + (part ? (unsigned long long)p.M : 0ull);
+        const unsigned j = (unsigned)n1 * (unsigned)p.S1 + col + (part ? (unsigned)p.M : 0u);
         const uint32_t *rw = seg + (part * L + n1) * K::SEGW4 + wi;
-        const uint64_t win = ((uint64_t)rw[0] | ((uint64_t)rw[1] << 32)) >> sh;
-        const int64_t r = (int64_t)((win >> 1) & mask);
-        const int64_t top = (j + 1 >= nd) ? 0 : (r >> (b - 1));
-        d[part] = j < nd ? (double)(r - (top << b) + (int64_t)(win & 1)) : 0.0;
+        // bits [sh, sh+32) of the 64-bit window: the bit below the digit, then
+        // its b <= 24 bits
+        const unsigned x = __funnelshift_r(rw[0], rw[1], sh);
+        const int r = (int)((x >> 1) & mask);
+        const int top = (j + 1 >= nd) ? 0 : (r >> (b - 1));
+        d[part] = j < nd ? (double)(r - (top << b) + (int)(x & 1u)) : 0.0;
       }
-      v[i] = cmul(make_double2(d[0], d[1]), __ldg(&p.pw_fwd[n1]));
+      v[i] = cmul(make_double2(d[0], d[1]), pwS[n1]);
     }
-    block_fft<L, W, false>(v, t, s, tile, p.twL1);
+    block_fft<L, W, false>(v, t, s, tile, twS);
     double2 w[PTS];
     outer_twiddles<TC>(p.tw4M, col, t, w);
 #pragma unroll
-    for (int i = 0; i < PTS; i++) gbuf[(uint64_t)(t + i * TC) * p.S1 + col] = cmul(v[i], w[i]);
+    for (int i = 0; i < PTS; i++) gbuf[(unsigned)(t + i * TC) * (unsigned)p.S1 + col] = cmul(v[i], w[i]);
     __syncthreads();
     st ^= 1;
   }
