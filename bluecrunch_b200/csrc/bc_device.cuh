@@ -144,15 +144,76 @@ template <int L, int W> struct TileSmem {
   static constexpr int elems = (W == 1) ? (L + L / 8) : (L * W);
 };
 
+// Per-stage twiddle tables for single-row transforms.  In a row transform
+// the lanes of a warp hold consecutive j, so a flat table read at
+// k*step (k = j mod NS) strides by multiples of 128 bytes and every lane of a
+// quarter-warp hits the same banks.  The staged layout stores, for each
+// radix-8 register stage with NS > 1, the twiddles w^1, w^2, w^4 it reads
+// for k = 0..NS-1 contiguously at offset(NS) + 3k.  The remainder stage
+// (radix 2 or 4) reads the flat table at k*r*L/(NS R) with consecutive k,
+// which is conflict-free already (and coalesced from global memory).
+template <int L> struct StagedTw {
+  using RX = Radices<L>;
+  static constexpr int NS0 = RX::has3 ? 3 : 1;
+  __host__ __device__ static constexpr int offset(int NS) {
+    int off = 0, ns = NS0;
+    for (int k = 0; k < RX::n8; k++, ns *= 8) {
+      if (ns == NS) return off;
+      if (ns > 1) off += ns * 3;
+    }
+    return off;
+  }
+  __host__ __device__ static constexpr int entries() {
+    int off = 0, ns = NS0;
+    for (int k = 0; k < RX::n8; k++, ns *= 8)
+      if (ns > 1) off += ns * 3;
+    return off > 0 ? off : 1;
+  }
+};
+
+// Fill a staged table from the flat one (flat[m] = e^{-2 pi i m/L}); all
+// threads of the CTA, published by the caller's next barrier.
+template <int L>
+__device__ __forceinline__ void staged_tw_build(double2 *dst, const double2 *__restrict__ flat) {
+  using ST = StagedTw<L>;
+  using RX = Radices<L>;
+  constexpr int n = ST::entries();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int off = 0, ns = ST::NS0, k = 0, e = 0;
+    bool found = false;
+    for (int st = 0; st < RX::n8; st++, ns *= 8) {
+      if (ns == 1) continue;
+      if (i < off + 3 * ns) {
+        k = (i - off) / 3;
+        e = (i - off) - 3 * k;
+        found = true;
+        break;
+      }
+      off += 3 * ns;
+    }
+    dst[i] = found ? flat[k * (1 << e) * (L / (ns * 8))] : make_double2(1.0, 0.0);
+  }
+}
+
+// Twiddle sources of a transform: `flat` (e^{-2 pi i m/L}, global or shared
+// memory) and, for STAGED transforms, the radix-8 stage tables.
+struct TwSrc {
+  const double2 *flat;
+  const double2 *staged;
+};
+
 // One register stage of radix R at span NS (Stockham, twiddle before the
-// butterfly: x_r *= w^{(j mod NS) r}, w = e^{-+2 pi i/(NS R)}).  tw[m] holds
-// e^{-2 pi i m/L} (global or shared memory); the largest m any stage reads
-// is below 3L/4 (radix 8 reads r*k*L/(8 NS) for r <= 4, radix 4 up to
-// 3*k*L/(4 NS), radix 2 k*L/(2 NS), k < NS), so tw_entries<L>() entries suffice.  Outputs stay in registers at v[q + r*(8/R)], whose
-// destination row is (j/NS)*NS*R + j%NS + r*NS.
-template <int L, int R, int NS, bool INV>
-__device__ __forceinline__ void reg_stage(double2 (&v)[PTS], int t, const double2 *__restrict__ tw) {
+// butterfly: x_r *= w^{(j mod NS) r}, w = e^{-+2 pi i/(NS R)}).  Flat
+// tables: tw[m] holds e^{-2 pi i m/L}; the largest m any stage reads is
+// below 3L/4 (radix 8 reads r*k*L/(8 NS) for r <= 4, radix 4 up to
+// 3*k*L/(4 NS), radix 2 k*L/(2 NS), k < NS), so tw_entries<L>() entries
+// suffice.  STAGED: radix-8 stages read StagedTw<L> tables.  Outputs stay in
+// registers at v[q + r*(8/R)], whose destination row is
+// (j/NS)*NS*R + j%NS + r*NS.
+template <int L, int R, int NS, bool INV, bool STAGED>
+__device__ __forceinline__ void reg_stage(double2 (&v)[PTS], int t, const TwSrc &ts) {
   constexpr int TC = L / PTS, Q = PTS / R;
+  const double2 *__restrict__ tw = ts.flat;
 #pragma unroll
   for (int q = 0; q < Q; q++) {
     const int j = t + q * TC;
@@ -164,7 +225,14 @@ __device__ __forceinline__ void reg_stage(double2 (&v)[PTS], int t, const double
       constexpr int step = L / (NS * R);
       if constexpr (R == 8) {
         // w^1, w^2, w^4 from the table, the other powers by one product each
-        const double2 w1 = tw[k * step], w2 = tw[2 * k * step], w4 = tw[4 * k * step];
+        double2 w1, w2, w4;
+        if constexpr (STAGED) {
+          constexpr int off = StagedTw<L>::offset(NS);
+          const double2 *b = ts.staged + off + 3 * k;
+          w1 = b[0]; w2 = b[1]; w4 = b[2];
+        } else {
+          w1 = tw[k * step]; w2 = tw[2 * k * step]; w4 = tw[4 * k * step];
+        }
         const double2 w3 = cmul(w1, w2), w5 = cmul(w1, w4), w6 = cmul(w2, w4), w7 = cmul(w3, w4);
         x[1] = ctw<INV>(x[1], w1); x[2] = ctw<INV>(x[2], w2); x[3] = ctw<INV>(x[3], w3);
         x[4] = ctw<INV>(x[4], w4); x[5] = ctw<INV>(x[5], w5); x[6] = ctw<INV>(x[6], w6);
@@ -237,31 +305,33 @@ __device__ __forceinline__ void smem_radix3_stage(int t, int s, double2 *sm, con
 }
 
 // Radix-8 stages k..n8-1, then the remainder stage; NS is the span so far.
-template <int L, int W, bool INV, int NS, int K, class Sync>
-__device__ __forceinline__ void run_pow2_stages(double2 (&v)[PTS], int t, int s, double2 *sm,
-                                                const double2 *__restrict__ tw, const Sync &sync) {
+template <int L, int W, bool INV, int NS, int K, bool STAGED, class Sync>
+__device__ __forceinline__ void run_pow2_stages(double2 (&v)[PTS], int t, int s, double2 *sm, const TwSrc &tw,
+                                                const Sync &sync) {
   using RX = Radices<L>;
   if constexpr (K < RX::n8) {
-    reg_stage<L, 8, NS, INV>(v, t, tw);
+    reg_stage<L, 8, NS, INV, STAGED>(v, t, tw);
     constexpr bool last = (K + 1 == RX::n8) && (RX::rem == 1);
     if constexpr (!last) {
       reg_stage_store<L, 8, NS, W>(v, t, s, sm);
       sync();
       load_regs<L, W>(v, t, s, sm);
       sync();
-      run_pow2_stages<L, W, INV, NS * 8, K + 1>(v, t, s, sm, tw, sync);
+      run_pow2_stages<L, W, INV, NS * 8, K + 1, STAGED>(v, t, s, sm, tw, sync);
     }
   } else if constexpr (RX::rem > 1) {
-    reg_stage<L, RX::rem, NS, INV>(v, t, tw);
+    reg_stage<L, RX::rem, NS, INV, STAGED>(v, t, tw);
   }
 }
-
 // Full block FFT.  v in/out per the register contract; sm is this tile's
-// shared memory; tw = e^{-2 pi i m/L}, m < tw_entries<L>().  Ends with the
+// shared memory; flat = e^{-2 pi i m/L}, m < tw_entries<L>().  STAGED: the
+// radix-8 stages read `staged` (StagedTw<L> layout) instead.  Ends with the
 // threads of the sync group past a barrier, so the group may reuse sm.
-template <int L, int W, bool INV, class Sync = CtaSync>
+template <int L, int W, bool INV, class Sync = CtaSync, bool STAGED = false>
 __device__ __forceinline__ void block_fft(double2 (&v)[PTS], int t, int s, double2 *sm,
-                                          const double2 *__restrict__ tw, const Sync &sync = Sync{}) {
+                                          const double2 *__restrict__ flat, const Sync &sync = Sync{},
+                                          const double2 *staged = nullptr) {
+  const TwSrc tw{flat, staged};
   using RX = Radices<L>;
   static_assert(L % PTS == 0, "block length must be a multiple of 8");
   if constexpr (RX::has3) {
@@ -270,9 +340,9 @@ __device__ __forceinline__ void block_fft(double2 (&v)[PTS], int t, int s, doubl
     smem_radix3_stage<L, W, INV>(t, s, sm, sync);
     load_regs<L, W>(v, t, s, sm);
     sync();
-    run_pow2_stages<L, W, INV, 3, 0>(v, t, s, sm, tw, sync);
+    run_pow2_stages<L, W, INV, 3, 0, STAGED>(v, t, s, sm, tw, sync);
   } else {
-    run_pow2_stages<L, W, INV, 1, 0>(v, t, s, sm, tw, sync);
+    run_pow2_stages<L, W, INV, 1, 0, STAGED>(v, t, s, sm, tw, sync);
   }
 }
 
@@ -404,8 +474,11 @@ __host__ __device__ __forceinline__ bool u192_is_ones(const U192 &h, int nbits) 
 __host__ __device__ __forceinline__ uint32_t u192_bits32(const U192 &h, int off) {
   if (off >= 192) return 0;
   const int wi = off >> 6, bi = off & 63;
-  unsigned long long lo = h.w[wi] >> bi;
-  if (bi > 32 && wi < 2) lo |= h.w[wi + 1] << (64 - bi);
+  // selects instead of a runtime word index, so h stays in registers
+  const unsigned long long a = wi == 0 ? h.w[0] : (wi == 1 ? h.w[1] : h.w[2]);
+  const unsigned long long b = wi == 0 ? h.w[1] : (wi == 1 ? h.w[2] : 0ull);
+  unsigned long long lo = a >> bi;
+  if (bi > 32) lo |= b << (64 - bi);
   return (uint32_t)lo;
 }
 

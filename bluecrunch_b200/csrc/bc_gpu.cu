@@ -9,6 +9,8 @@
 // width table, scratch comes from one device arena, and every failure is a
 // status code.
 #include <algorithm>
+#include <thread>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -56,7 +58,7 @@ bool shape_for(size_t M, Shape &s) {
   for (int L1 : kOuterLens) {
     if (M % L1) continue;
     const size_t Lr = M / L1;
-    if (is_row_len(Lr) && pow2part(Lr) >= (size_t)std::max(8, 2048 / L1)) {
+    if (is_row_len(Lr) && pow2part(Lr) >= (size_t)pass_tile_w(L1)) {
       s.M = (int)M; s.L1 = L1; s.L2 = 1; s.Lr = (int)Lr; s.levels = 2; return true;
     }
   }
@@ -71,7 +73,7 @@ bool shape_for(size_t M, Shape &s) {
       if (R % L1) continue;
       const size_t L2 = R / L1;
       if (L2 < 64 || L2 > 512 || (L2 & (L2 - 1)) || L2 > (size_t)L1) continue;
-      if (pow2part(Lr) < (size_t)std::max(8, 2048 / (int)L2) || pow2part(L2 * Lr) < (size_t)std::max(8, 2048 / L1)) continue;
+      if (pow2part(Lr) < (size_t)pass_tile_w((int)L2) || pow2part(L2 * Lr) < (size_t)pass_tile_w(L1)) continue;
       s.M = (int)M; s.L1 = L1; s.L2 = (int)L2; s.Lr = (int)Lr; s.levels = 3; return true;
     }
   }
@@ -497,11 +499,22 @@ int encode_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dim
 // TMA boxes must deliver exactly the bytes its kernel waits for, boxes must
 // tile the rows, and column tiles must tile the rows of each pass.  Checked
 // before every launch and, for all lengths, by bc_gpu_check_shapes.
+// Dynamic shared memory a CTA may use on sm_100 (227 KB).
+constexpr size_t kMaxSmemPerCta = 227 * 1024;
+
 bool shape_launch_ok(const Shape &s, bool sq) {
-  if (s.levels == 1) return get_small(s.M, sq).fn != nullptr;
+  if (s.levels == 1) {
+    const KInfo k = get_small(s.M, sq);
+    return k.fn != nullptr && k.smem <= kMaxSmemPerCta;
+  }
   const size_t S1 = s.M / s.L1, Lr = s.levels == 3 ? (size_t)s.Lr : S1;
   KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true), kr = get_rows((int)Lr, sq);
   if (!ko.fn || !ki.fn || !kr.fn) return false;
+  if (ko.smem > kMaxSmemPerCta || ki.smem > kMaxSmemPerCta || kr.smem > kMaxSmemPerCta) return false;
+  if (s.levels == 3) {
+    const KInfo kmf = get_mid(s.L2, false), kmi = get_mid(s.L2, true);
+    if (!kmf.fn || !kmi.fn || kmf.smem > kMaxSmemPerCta || kmi.smem > kMaxSmemPerCta) return false;
+  }
   const int W1 = ko.threads / (s.L1 / PTS);
   if (S1 % W1 || W1 % 8) return false;
   if ((size_t)(W1 / 8) * ki.parts * 128 * ki.box != ki.unit_bytes || (size_t)ki.box * ki.parts != (size_t)s.L1)
@@ -618,14 +631,58 @@ int arena_reserve(size_t bytes) {
   return BC_OK;
 }
 
-bool is_device_ptr(const void *p) {
-  if (!p) return false;
+enum MemKind { MEM_PAGEABLE = 0, MEM_PINNED = 1, MEM_DEVICE = 2 };
+MemKind mem_kind(const void *p) {
+  if (!p) return MEM_PAGEABLE;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return MEM_PAGEABLE;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return MEM_DEVICE;
+  return a.type == cudaMemoryTypeHost ? MEM_PINNED : MEM_PAGEABLE;
+}
+bool is_device_ptr(const void *p) { return mem_kind(p) == MEM_DEVICE; }
+
+// Host memcpy of many arrays on up to $BC_COPY_THREADS (default: all
+// hardware threads, at most 32) threads, in pieces of at least 1 MiB.
+struct CopyJob {
+  char *dst;
+  const char *src;
+  size_t n;
+};
+unsigned copy_threads() {
+  static unsigned n = [] {
+    unsigned t = std::thread::hardware_concurrency();
+    if (const char *e = getenv("BC_COPY_THREADS")) t = (unsigned)atoi(e);
+    return std::max(1u, std::min(t ? t : 1u, 32u));
+  }();
+  return n;
+}
+void par_copy(const std::vector<CopyJob> &jobs) {
+  size_t total = 0;
+  for (const CopyJob &j : jobs) total += j.n;
+  const unsigned nt = (unsigned)std::min<size_t>(copy_threads(), total / (size_t(4) << 20) + 1);
+  if (nt <= 1) {
+    for (const CopyJob &j : jobs) memcpy(j.dst, j.src, j.n);
+    return;
+  }
+  const size_t piece = std::max<size_t>(size_t(1) << 20, total / (4 * nt));
+  std::vector<CopyJob> pieces;
+  for (const CopyJob &j : jobs) {
+    if (j.n <= piece) { pieces.push_back(j); continue; }
+    for (size_t o = 0; o < j.n; o += piece) pieces.push_back({j.dst + o, j.src + o, std::min(piece, j.n - o)});
+  }
+  std::atomic<size_t> next{0};
+  auto worker = [&] {
+    for (size_t i; (i = next.fetch_add(1, std::memory_order_relaxed)) < pieces.size();)
+      memcpy(pieces[i].dst, pieces[i].src, pieces[i].n);
+  };
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  for (unsigned k = 1; k < nt; k++) th.emplace_back(worker);
+  worker();
+  for (std::thread &t : th) t.join();
 }
 
 // ------------------------------------------------------------------ batch core
@@ -656,23 +713,54 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-// Run one attempt over `works` (all not done).  Fills err/flags.
-// Pinned host staging for small operands and results: one host-to-device
-// and one device-to-host copy per batch instead of one per item.
-constexpr size_t kStageItemMax = size_t(1) << 20;  // bytes; larger arrays copy directly
-
+// Pageable host operands and results go through pinned staging buffers: one
+// host-to-device and one device-to-host copy per batch instead of one per
+// item, filled and drained by par_copy.  Pinned host arrays copy directly.
 struct PinnedStage {
   char *p = nullptr;
   size_t cap = 0;
 };
 PinnedStage g_pin_in, g_pin_out;
 
+// Host-side phase times of the batch path, printed at exit when $BC_PROFILE
+// is set (seconds).
+struct HostProfile {
+  double plan = 0, layout = 0, pin_alloc = 0, copy_in = 0, launch = 0, wait = 0, copy_out = 0;
+  size_t calls = 0, items = 0, bytes_in = 0, bytes_out = 0;
+};
+HostProfile g_prof;
+double g_prof_rest = 0;  // time outside the phases above
+bool g_prof_on = false;
+void print_profile() {
+  const HostProfile &h = g_prof;
+  fprintf(stderr,
+          "bc_gpu profile: %zu batch calls, %zu items, in %.2f GB, out %.2f GB, %u copy threads\n"
+          "  plan %.3f s, layout %.3f s, pinned alloc %.3f s, copy in %.3f s, launch %.3f s, "
+          "wait %.3f s, copy out %.3f s\n",
+          h.calls, h.items, h.bytes_in / 1e9, h.bytes_out / 1e9, copy_threads(), h.plan, h.layout, h.pin_alloc,
+          h.copy_in, h.launch, h.wait, h.copy_out);
+}
+// Adds the time since construction (or the last next()) to *acc.
+struct PhaseTimer {
+  double *acc;
+  std::chrono::steady_clock::time_point t0;
+  explicit PhaseTimer(double *a) : acc(a), t0(std::chrono::steady_clock::now()) {}
+  void next(double *a) {
+    auto t = std::chrono::steady_clock::now();
+    *acc += std::chrono::duration<double>(t - t0).count();
+    t0 = t;
+    acc = a;
+  }
+  ~PhaseTimer() { next(acc); }
+};
+
 int pinned_reserve(PinnedStage &ps, size_t bytes) {
   if (bytes <= ps.cap) return BC_OK;
+  PhaseTimer pt(&g_prof.pin_alloc);
   if (ps.p) CK(cudaFreeHost(ps.p));
   ps.p = nullptr;
   ps.cap = 0;
-  size_t want = std::max(bytes + bytes / 2, (size_t)1 << 22);
+  size_t want = std::max(2 * bytes, (size_t)1 << 26);  // doubling: few reallocations
   CK(cudaHostAlloc((void **)&ps.p, want, cudaHostAllocDefault));
   ps.cap = want;
   return BC_OK;
@@ -683,6 +771,9 @@ int pinned_reserve(PinnedStage &ps, size_t bytes) {
 int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st, unsigned flags_in) {
   const bool all_host = flags_in & BC_BATCH_HOST_OPERANDS;
   const size_t nw = works.size();
+  double scratch = 0;
+  PhaseTimer pt(&g_prof.layout);
+  g_prof.items += nw;
   // ---- classes (M, square); items of a class get contiguous slabs
   std::map<std::pair<size_t, bool>, std::vector<size_t>> classes;
   for (size_t i = 0; i < nw; i++) classes[{(size_t)works[i]->pl.shape.M, works[i]->pl.square}].push_back(i);
@@ -697,15 +788,18 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   for (size_t i = 0; i < nw; i++) {
     const bc_mul_desc &d = items[works[i]->idx];
     const Plan &pl = works[i]->pl;
-    hostA[i] = pl.AL && (all_host || !is_device_ptr(d.A));
-    hostB[i] = !pl.square && pl.BL && (all_host || !is_device_ptr(d.B));
-    runs[i].hostC = all_host || !is_device_ptr(d.C);
+    const MemKind ka = all_host ? MEM_PAGEABLE : mem_kind(d.A);
+    const MemKind kb = pl.square ? ka : (all_host ? MEM_PAGEABLE : mem_kind(d.B));
+    const MemKind kc = all_host ? MEM_PAGEABLE : mem_kind(d.C);
+    hostA[i] = pl.AL && ka != MEM_DEVICE;
+    hostB[i] = !pl.square && pl.BL && kb != MEM_DEVICE;
+    runs[i].hostC = kc != MEM_DEVICE;
     runs[i].stagedC = !runs[i].hostC && (overlaps(d.C, d.CL * 4, d.A, d.AL * 4) || overlaps(d.C, d.CL * 4, d.B, d.BL * 4));
-    slots[i].off_dA = off; if (hostA[i]) off += align256(pl.AL * 4);
-    slots[i].off_dB = off; if (hostB[i]) off += align256(pl.BL * 4);
-    if (hostA[i] && pl.AL * 4 <= kStageItemMax) { pin_in_off[i] = stage_in; stage_in += align256(pl.AL * 4); }
-    if (hostB[i] && pl.BL * 4 <= kStageItemMax) { pin_inB_off[i] = stage_in; stage_in += align256(pl.BL * 4); }
-    if (runs[i].hostC && d.CL * 4 <= kStageItemMax) { pin_out_off[i] = stage_out; stage_out += align256(d.CL * 4); }
+    if (hostA[i] && ka == MEM_PAGEABLE) { pin_in_off[i] = stage_in; stage_in += align256(pl.AL * 4); }
+    if (hostB[i] && kb == MEM_PAGEABLE) { pin_inB_off[i] = stage_in; stage_in += align256(pl.BL * 4); }
+    if (runs[i].hostC && kc == MEM_PAGEABLE) { pin_out_off[i] = stage_out; stage_out += align256(d.CL * 4); }
+    slots[i].off_dA = off; if (hostA[i] && pin_in_off[i] == SIZE_MAX) off += align256(pl.AL * 4);
+    slots[i].off_dB = off; if (hostB[i] && pin_inB_off[i] == SIZE_MAX) off += align256(pl.BL * 4);
     slots[i].off_dC = off;
     if ((runs[i].hostC && pin_out_off[i] == SIZE_MAX) || runs[i].stagedC) off += align256(d.CL * 4);
   }
@@ -746,15 +840,22 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   char *base = g.arena;
 
   // ---- inputs
+  pt.next(&g_prof.copy_in);
   if (stage_in) {
+    pt.next(&scratch);
     if ((r = pinned_reserve(g_pin_in, stage_in))) return r;
+    pt.next(&g_prof.copy_in);
+    std::vector<CopyJob> jobs;
+    jobs.reserve(2 * nw);
     for (size_t i = 0; i < nw; i++) {
       const bc_mul_desc &d = items[works[i]->idx];
-      if (pin_in_off[i] != SIZE_MAX) memcpy(g_pin_in.p + pin_in_off[i], d.A, works[i]->pl.AL * 4);
-      if (pin_inB_off[i] != SIZE_MAX) memcpy(g_pin_in.p + pin_inB_off[i], d.B, works[i]->pl.BL * 4);
+      if (pin_in_off[i] != SIZE_MAX) jobs.push_back({g_pin_in.p + pin_in_off[i], (const char *)d.A, works[i]->pl.AL * 4});
+      if (pin_inB_off[i] != SIZE_MAX) jobs.push_back({g_pin_in.p + pin_inB_off[i], (const char *)d.B, works[i]->pl.BL * 4});
     }
+    par_copy(jobs);
     CK(cudaMemcpyAsync(base + off_stage_in, g_pin_in.p, stage_in, cudaMemcpyHostToDevice, g.stream));
     st->h2d_bytes += stage_in;
+    g_prof.bytes_in += stage_in;
   }
   for (size_t i = 0; i < nw; i++) {
     const bc_mul_desc &d = items[works[i]->idx];
@@ -823,6 +924,7 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   unsigned int *ctr = (unsigned int *)(base + off_ctr);
 
   // ---- launches
+  pt.next(&g_prof.launch);
   CK(cudaEventRecord(g.ev0, g.stream));
   size_t first = 0, cls = 0;
   for (auto &c : classes) {
@@ -856,7 +958,9 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   std::vector<unsigned> flags(nw);
   CK(cudaMemcpyAsync(errs.data(), base + off_err, nw * 8, cudaMemcpyDeviceToHost, g.stream));
   CK(cudaMemcpyAsync(flags.data(), base + off_flags, nw * 4, cudaMemcpyDeviceToHost, g.stream));
+  pt.next(&g_prof.wait);
   CK(cudaStreamSynchronize(g.stream));
+  pt.next(&g_prof.copy_out);
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, g.ev0, g.ev1));
   st->device_ms += ms;
@@ -871,7 +975,11 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     for (auto e : g.kev) cudaEventDestroy(e);
     g.kev.clear();
   }
-  if (stage_out && (r = pinned_reserve(g_pin_out, stage_out))) return r;
+  if (stage_out) {
+    pt.next(&scratch);
+    if ((r = pinned_reserve(g_pin_out, stage_out))) return r;
+    pt.next(&g_prof.copy_out);
+  }
   bool copies = false, staged_out = false;
   std::vector<char> ok(nw);
   for (size_t i = 0; i < nw; i++) {
@@ -898,11 +1006,17 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   if (staged_out) {
     CK(cudaMemcpyAsync(g_pin_out.p, base + off_stage_out, stage_out, cudaMemcpyDeviceToHost, g.stream));
     st->d2h_bytes += stage_out;
+    g_prof.bytes_out += stage_out;
   }
   if (copies) CK(cudaStreamSynchronize(g.stream));
-  if (staged_out)
+  if (staged_out) {
+    std::vector<CopyJob> jobs;
+    jobs.reserve(nw);
     for (size_t i = 0; i < nw; i++)
-      if (ok[i] && pin_out_off[i] != SIZE_MAX) memcpy(items[works[i]->idx].C, g_pin_out.p + pin_out_off[i], items[works[i]->idx].CL * 4);
+      if (ok[i] && pin_out_off[i] != SIZE_MAX)
+        jobs.push_back({(char *)items[works[i]->idx].C, g_pin_out.p + pin_out_off[i], items[works[i]->idx].CL * 4});
+    par_copy(jobs);
+  }
   return BC_OK;
 }
 
@@ -911,8 +1025,10 @@ int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Pla
   if (!g.init) return fail(BC_ERR_NOT_INIT);
   if (n && !items) return fail(BC_ERR_INVALID);
   auto t0 = std::chrono::steady_clock::now();
+  g_prof.calls++;
   std::vector<Work> works;
   works.reserve(n);
+  PhaseTimer ppt(&g_prof.plan);
   for (size_t i = 0; i < n; i++) {
     const bc_mul_desc &d = items[i];
     if (d.CL && !d.C) return fail(BC_ERR_INVALID);
@@ -932,6 +1048,7 @@ int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Pla
     works.push_back(w);
   }
   st->items = n;
+  ppt.next(&g_prof_rest);  // the attempts are timed inside run_attempt
   if (g.time_kernels) g.ktimes.clear();
   // attempts: redo items whose rounding error reached the limit at a narrower width
   for (int attempt = 0; attempt < 12; attempt++) {
@@ -1011,6 +1128,10 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
   CK(cudaMemGetInfo(&fre, &tot));
   g.arena_limit = c.arena_bytes ? c.arena_bytes : (size_t)(fre * 0.9);
   g.max_err = c.max_round_err > 0 ? c.max_round_err : 0.25;
+  if (getenv("BC_PROFILE") && !g_prof_on) {
+    g_prof_on = true;
+    atexit(print_profile);
+  }
   g.verbose = c.verbose || getenv("BC_VERBOSE") != nullptr;
   load_width_file(c.tune_path);
   g.init = true;

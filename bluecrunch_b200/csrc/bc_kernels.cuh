@@ -101,10 +101,14 @@ __device__ __forceinline__ void atomic_max_err(unsigned long long *p, double e) 
 // ------------------------------------------------------------------ runs
 // 8 consecutive rounded coefficients c_u (exact integers held in doubles) ->
 // H = sum (bits of the running carry) and C = final signed carry.
+// h |= bits << off for off < 192 (selects instead of a runtime word index,
+// so h stays in registers).
 __host__ __device__ __forceinline__ void u192_or_bits(U192 &h, unsigned long long bits, int off) {
   const int wi = off >> 6, bi = off & 63;
-  h.w[wi] |= bits << bi;
-  if (bi && wi < 2) h.w[wi + 1] |= bits >> (64 - bi);
+  const unsigned long long lo = bits << bi, hi = bi ? bits >> (64 - bi) : 0ull;
+  h.w[0] |= wi == 0 ? lo : 0ull;
+  h.w[1] |= wi == 1 ? lo : (wi == 0 ? hi : 0ull);
+  h.w[2] |= wi == 2 ? lo : (wi == 1 ? hi : 0ull);
 }
 
 __host__ __device__ __forceinline__ RunRec make_run(const double *c, int b) {

@@ -17,14 +17,28 @@
 
 namespace bc {
 
-// Tile width (columns) of an L-row pass tile: 2048 points, at least 8 columns.
+// Points per unit of the column passes and of the row pass.
+#ifndef BC_PASS_POINTS
+#define BC_PASS_POINTS 1024
+#endif
+#ifndef BC_ROW_POINTS
+#define BC_ROW_POINTS 1024
+#endif
+
+// Tile width (columns) of an L-row pass tile: BC_PASS_POINTS points, at
+// least 8 columns (one 128-byte swizzle atom).
+__host__ __device__ constexpr int pass_tile_w(int L) {
+  return (BC_PASS_POINTS / L) >= 8 ? BC_PASS_POINTS / L : 8;
+}
+
 template <int L> struct PassTile {
-  static constexpr int W = (2048 / L) >= 8 ? 2048 / L : 8;
+  static constexpr int W = pass_tile_w(L);
   static constexpr int NT = (L / PTS) * W;
   static constexpr int BOX_ROWS = L > 256 ? 256 : L;
   static constexpr int HALVES = L / BOX_ROWS;
   static constexpr unsigned BYTES = (unsigned)L * W * 16;
-  static constexpr int MINB = NT <= 256 ? 2 : 1;  // resident CTAs per SM the register budget allows for
+  // resident CTAs per SM with at most 128 registers per thread
+  static constexpr int MINB = NT >= 512 ? 1 : 512 / NT;
   static constexpr int TWN = tw_entries<L>();     // L-point stage twiddles kept in shared memory
   // dynamic shared memory of k2_mid / k2_outer_inv: two tiles, the stage
   // twiddles, the outer pass's weights (outer_inv only), 1024 bytes of slack
@@ -252,8 +266,8 @@ constexpr int pow2_floor(int x) { return x >= 2 ? 2 * pow2_floor(x / 2) : 1; }
 
 template <int L> struct RowTile {
   // rows per unit: a power of two (so units never straddle items, whose row
-  // counts are powers of two) with about 2048 points per operand
-  static constexpr int NR = pow2_floor(2048 / L > 0 ? 2048 / L : 1);
+  // counts are powers of two) with about BC_ROW_POINTS points per operand
+  static constexpr int NR = pow2_floor(BC_ROW_POINTS / L > 0 ? BC_ROW_POINTS / L : 1);
   static constexpr int NT = (L / PTS) * NR;
   static constexpr int LINES = L / 8;
   // TMA boxes hold at most 256 lines: split a row into equal boxes
@@ -261,11 +275,14 @@ template <int L> struct RowTile {
   static constexpr int BOX_LINES = LINES / PARTS;
   static_assert(BOX_LINES * PARTS == LINES && BOX_LINES % 8 == 0, "row split into whole swizzle atoms");
   static_assert(PARTS == 1 || NR == 1, "split rows come one per unit");
-  static constexpr int MINB = NT <= 256 ? 2 : 1;
-  // stage twiddles in shared memory where two CTAs per SM still fit
-  static constexpr bool TWS = L <= 1536;
-  static constexpr int TWN = TWS ? tw_entries<L>() : 0;
-  static constexpr size_t SMEM = 3 * (size_t)NR * L * 16 + (size_t)TWN * 16 + 1024;
+  static constexpr int MINB = NT <= 128 ? 3 : (NT <= 256 ? 2 : 1);
+  static constexpr size_t TILE = (size_t)NR * L * 16;  // one operand's rows of a unit
+  // radix-8 stage twiddles in shared memory (staged layout)
+  static constexpr int TWN = StagedTw<L>::entries();
+  // slots per operand: two (the next unit loads while one is transformed)
+  // when four tiles fit the 227 KB a CTA may use, else one
+  static constexpr int SLOTS = (4 * TILE + (size_t)TWN * 16 + 1024 <= 227 * 1024) ? 2 : 1;
+  static constexpr size_t SMEM = 2 * SLOTS * TILE + (size_t)TWN * 16 + 1024;
 };
 
 // Barrier of one row's L/8 threads inside k2_rows: a named barrier when the
@@ -292,86 +309,91 @@ __device__ __forceinline__ void rows_load(double2 *dst, const CUtensorMap *map, 
   }
 }
 
+// Buffers: A and B each have SLOTS slots (two where they fit), so the rows
+// of unit u + SLOTS*grid load while unit u is transformed.  A's spectrum
+// stays in its own slot; B's slot is free after the product, A's after the
+// inverse transform (which exchanges through A's slot).  Squaring uses the
+// A slots only.
 template <int L, bool SQ>
 __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
     k2_rows(ClassParams p, const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB) {
   using R = RowTile<L>;
-  constexpr int TC = L / PTS, NR = R::NR;
+  constexpr int TC = L / PTS, NR = R::NR, NS = R::SLOTS;
   extern __shared__ unsigned char smraw[];
-  __shared__ uint64_t bars[2];  // 0: A buffer, 1: B buffer
-  double2 *bufA = align1024(smraw);
-  double2 *bufB = bufA + NR * L;
-  double2 *bufS = bufB + NR * L;  // A's spectrum while B is transformed
-  const double2 *tw = p.twLr;
-  if constexpr (R::TWS) {
-    double2 *twS = bufS + NR * L;
-    table_to_smem(twS, p.twLr, R::TWN);
-    tw = twS;
-  }
+  __shared__ uint64_t bars[4];  // A slot q: bars[q]; B slot q: bars[2 + q]
+  double2 *const bufA0 = align1024(smraw);  // A slot q at bufA0 + q*NR*L, B slot q at bufA0 + (NS+q)*NR*L
+  double2 *twS = bufA0 + 2 * NS * NR * L;
+  staged_tw_build<L>(twS, p.twLr);
   const int tid = threadIdx.x, rl = tid / TC, t = tid % TC;
   const unsigned rows_item = p.M / L;
   const unsigned total = (unsigned)p.nitems * rows_item / NR;  // far below 2^32
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+#pragma unroll
+    for (int k = 0; k < 4; k++) mbar_init(&bars[k], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  unsigned phA = 0, phB = 0;
   unsigned u = blockIdx.x;
-  if (tid == 0 && u < total) {
+  if (tid == 0) {
     fence_proxy_async_smem();
-    rows_load<L>(bufA, &mA, &bars[0], u * NR);
-    if (!SQ) rows_load<L>(bufB, &mB, &bars[1], u * NR);
+#pragma unroll
+    for (int q = 0; q < NS; q++) {
+      const unsigned uq = u + q * gridDim.x;
+      if (uq < total) {
+        rows_load<L>(bufA0 + q * NR * L, &mA, &bars[q], uq * NR);
+        if (!SQ) rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], uq * NR);
+      }
+    }
   }
-  double2 *smA = bufA + rl * L, *smB = bufB + rl * L, *smS = bufS + rl * L;
-  const auto rsync = RowSyncOf<L>::make(rl);  // the threads of this row
-  for (; u < total; u += gridDim.x) {
-    const unsigned un = u + gridDim.x;
-    const unsigned grow = u * NR + rl;  // this thread's row in the class slab
+  using RS = typename RowSyncOf<L>::type;
+  const RS rsync = RowSyncOf<L>::make(rl);  // the threads of this row
+  unsigned phases = 0;                      // bit k: parity to wait for on bars[k]
+  for (int q = 0; u < total; u += gridDim.x, q = (q + 1 == NS) ? 0 : q + 1) {
+    const unsigned un = u + NS * gridDim.x;  // the unit this slot loads next
+    const unsigned grow = u * NR + rl;        // this thread's row in the class slab
     const unsigned item = grow / rows_item;
     const ItemDesc &it = p.items[item];
     double2 *ra = it.bufA + (grow - item * rows_item) * (unsigned)L;
+    double2 *smA = bufA0 + q * NR * L + rl * L;
+    double2 *smB = bufA0 + (NS + q) * NR * L + rl * L;
     double2 v[PTS];
-    bool ok = mbar_wait(&bars[0], phA);
-    phA ^= 1;
+    bool ok = mbar_wait(&bars[q], (phases >> q) & 1u);
+    phases ^= 1u << q;
     if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
 #pragma unroll
     for (int i = 0; i < PTS; i++) v[i] = smA[ridx(t + i * TC)];
     rsync();
-    block_fft<L, 1, false>(v, t, 0, smA, tw, rsync);
+    block_fft<L, 1, false, RS, true>(v, t, 0, smA, p.twLr, rsync, twS);
     if (SQ) {
 #pragma unroll
       for (int i = 0; i < PTS; i++) v[i] = cmul(v[i], v[i]);
+      rsync();  // the inverse overwrites entries other threads of the row may still read
     } else {
 #pragma unroll
-      for (int i = 0; i < PTS; i++) smS[ridx(t + i * TC)] = v[i];  // read back by this thread only
-    }
-    __syncthreads();
-    if (tid == 0 && un < total) {  // A's buffer is free: fetch the next rows of A
-      fence_proxy_async_smem();
-      rows_load<L>(bufA, &mA, &bars[0], un * NR);
-    }
-    if (!SQ) {
-      ok = mbar_wait(&bars[1], phB);
-      phB ^= 1;
+      for (int i = 0; i < PTS; i++) smA[ridx(t + i * TC)] = v[i];  // A's spectrum, read back by this thread only
+      ok = mbar_wait(&bars[2 + q], (phases >> (2 + q)) & 1u);
+      phases ^= 1u << (2 + q);
       if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
 #pragma unroll
       for (int i = 0; i < PTS; i++) v[i] = smB[ridx(t + i * TC)];
       rsync();
-      block_fft<L, 1, false>(v, t, 0, smB, tw, rsync);
+      block_fft<L, 1, false, RS, true>(v, t, 0, smB, p.twLr, rsync, twS);
 #pragma unroll
-      for (int i = 0; i < PTS; i++) v[i] = cmul(smS[ridx(t + i * TC)], v[i]);
-      __syncthreads();  // every row is done with B's buffer and with its spectrum reads
-      if (tid == 0 && un < total) {  // fetch the next rows of B during the inverse
+      for (int i = 0; i < PTS; i++) v[i] = cmul(smA[ridx(t + i * TC)], v[i]);
+      __syncthreads();  // every row is done with this B slot and with its spectrum reads
+      if (tid == 0 && un < total) {
         fence_proxy_async_smem();
-        rows_load<L>(bufB, &mB, &bars[1], un * NR);
+        rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], un * NR);
       }
     }
-    // the inverse exchanges through the spectrum buffer, private to the row
-    block_fft<L, 1, true>(v, t, 0, smS, tw, rsync);
+    block_fft<L, 1, true, RS, true>(v, t, 0, smA, p.twLr, rsync, twS);
 #pragma unroll
     for (int i = 0; i < PTS; i++) ra[t + i * TC] = v[i];
+    __syncthreads();  // every row is done with this A slot
+    if (tid == 0 && un < total) {
+      fence_proxy_async_smem();
+      rows_load<L>(bufA0 + q * NR * L, &mA, &bars[q], un * NR);
+    }
   }
 }
 

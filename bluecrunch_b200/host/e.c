@@ -17,6 +17,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "bc_host.h"
 #include "bench.h"
@@ -67,7 +68,15 @@ typedef struct {
   _bigfloat_struct P, Q;
 } bnode;
 
+static double wall_s(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
 static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
+  const int stats = getenv("BC_STATS") != NULL;
+  double t_leaf = 0, t_mul = 0, t_add = 0, t0 = wall_s();
   /* top-down: the tree above the host subtrees, one array per depth */
   bnode **lv = (bnode **)bc_xmalloc(sizeof(bnode *));
   size_t *cnt = (size_t *)bc_xmalloc(sizeof(size_t));
@@ -110,6 +119,7 @@ static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
       bsr(&x->P, &x->Q, x->a, x->b);
     }
   }
+  t_leaf = wall_s() - t0;
   /* bottom-up: one batch of 2 products per internal node, then the adds */
   for (int d = nlv - 2; d >= 0; d--) {
     bnode *L = lv[d], *N = lv[d + 1];
@@ -128,7 +138,10 @@ static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
       it[j].target = &tmp[j / 2]; it[j].a = &l->P; it[j].b = &r->Q; it[j].p = 0; j++;  /* P0*Q1 */
       it[j].target = &x->Q;       it[j].a = &l->Q; it[j].b = &r->Q; it[j].p = 0; j++;  /* Q0*Q1 */
     }
+    t0 = wall_s();
     bigfloat_mul_batch(it, j);
+    t_mul += wall_s() - t0;
+    t0 = wall_s();
     free(it);
     long mm = (long)m;
     j = 0;
@@ -146,7 +159,11 @@ static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
     free(slot);
     free(tmp);
     free(N);
+    t_add += wall_s() - t0;
   }
+  if (stats)
+    printf("    binary splitting: host subtrees %.3f s, level products %.3f s, adds and frees %.3f s\n", t_leaf,
+           t_mul, t_add);
   free(P->coef);
   free(Q->coef);
   *P = lv[0][0].P;
