@@ -76,6 +76,9 @@ GPU_SYMBOLS = {
                                   ctypes.POINTER(MulStats)]),
     "bc_gpu_mul_batch": (ctypes.c_int, [ctypes.POINTER(MulDesc), _sz, ctypes.POINTER(BatchStats)]),
     "bc_gpu_mul_batch_flags": (ctypes.c_int, [ctypes.POINTER(MulDesc), _sz, ctypes.c_uint, ctypes.POINTER(BatchStats)]),
+    "bc_gpu_e_series": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
+                                       ctypes.POINTER(_sz), ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
+                                       ctypes.POINTER(_sz)]),
     "bc_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p]),
     "bc_gpu_plan": (ctypes.c_int, [_sz, _sz, _sz, ctypes.c_int, ctypes.POINTER(PlanInfo)]),
     "bc_gpu_width_limit": (ctypes.c_int, [_sz]),

@@ -25,6 +25,7 @@
 
 #include "bc_gpu.h"
 #include "bc_pipe.cuh"
+#include "bc_bsr.cuh"
 
 using namespace bc;
 
@@ -770,6 +771,7 @@ int pinned_reserve(PinnedStage &ps, size_t bytes) {
 // out the products that pass the rounding check.
 int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st, unsigned flags_in) {
   const bool all_host = flags_in & BC_BATCH_HOST_OPERANDS;
+  const bool all_dev = flags_in & BC_BATCH_DEVICE_OPERANDS;
   const size_t nw = works.size();
   double scratch = 0;
   PhaseTimer pt(&g_prof.layout);
@@ -788,9 +790,9 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   for (size_t i = 0; i < nw; i++) {
     const bc_mul_desc &d = items[works[i]->idx];
     const Plan &pl = works[i]->pl;
-    const MemKind ka = all_host ? MEM_PAGEABLE : mem_kind(d.A);
-    const MemKind kb = pl.square ? ka : (all_host ? MEM_PAGEABLE : mem_kind(d.B));
-    const MemKind kc = all_host ? MEM_PAGEABLE : mem_kind(d.C);
+    const MemKind ka = all_dev ? MEM_DEVICE : all_host ? MEM_PAGEABLE : mem_kind(d.A);
+    const MemKind kb = pl.square ? ka : (all_dev ? MEM_DEVICE : all_host ? MEM_PAGEABLE : mem_kind(d.B));
+    const MemKind kc = all_dev ? MEM_DEVICE : all_host ? MEM_PAGEABLE : mem_kind(d.C);
     hostA[i] = pl.AL && ka != MEM_DEVICE;
     hostB[i] = !pl.square && pl.BL && kb != MEM_DEVICE;
     runs[i].hostC = kc != MEM_DEVICE;
@@ -1036,7 +1038,8 @@ int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Pla
     if (d.CL == 0) continue;
     const bool zero = d.AL == 0 || d.BL == 0;
     if (zero) {
-      if (!(flags & BC_BATCH_HOST_OPERANDS) && is_device_ptr(d.C)) CK(cudaMemsetAsync(d.C, 0, d.CL * 4, g.stream));
+      if ((flags & BC_BATCH_DEVICE_OPERANDS) || (!(flags & BC_BATCH_HOST_OPERANDS) && is_device_ptr(d.C)))
+        CK(cudaMemsetAsync(d.C, 0, d.CL * 4, g.stream));
       else memset(d.C, 0, d.CL * 4);
       continue;
     }
@@ -1095,6 +1098,150 @@ int mul_batch_locked(const bc_mul_desc *items, size_t n, bc_batch_stats *st, Pla
     if (!w.done) return fail(BC_ERR_PRECISION);
   if (first_plan && !works.empty()) *first_plan = works[0].pl;
   st->total_ms += ms_since(t0);
+  return BC_OK;
+}
+
+// ------------------------------------------------------------------ e's series on the device
+// Binary splitting of sum 1/k! with every value kept in device memory: the
+// leaves (LEAF_TERMS terms each) by k_bsr_leaves, then one level at a time
+// the products P_l*Q_r and Q_l*Q_r of neighbouring nodes in one batch
+// (device operands), their lengths by k_trim and P = P_l*Q_r + P_r by k_add.
+// Only the lengths cross to the host between steps; P and Q of the root at
+// the end.
+struct DevNum {
+  uint32_t *p = nullptr;
+  size_t len = 0;
+};
+
+struct DevBuf {  // cudaMalloc'd, freed on scope exit
+  void *p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+  int alloc(size_t bytes) {
+    CK(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+    return BC_OK;
+  }
+};
+
+int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vector<uint32_t> &hQ,
+                    bc_batch_stats *st) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (b <= a || b > 0xfffffff0u) return fail(BC_ERR_INVALID);
+  const uint32_t nleaf = (b - a + LEAF_TERMS - 1) / LEAF_TERMS;
+  DevBuf level, lens;
+  int r;
+  if ((r = level.alloc((size_t)nleaf * 2 * LEAF_STRIDE * 4)) || (r = lens.alloc((size_t)nleaf * 2 * 4))) return r;
+  k_bsr_leaves<<<(nleaf + LEAF_NT - 1) / LEAF_NT, LEAF_NT, 0, g.stream>>>(a, b, nleaf, (uint32_t *)level.p,
+                                                                        (uint32_t *)lens.p);
+  CK(cudaGetLastError());
+  std::vector<uint32_t> l0(2 * (size_t)nleaf);
+  CK(cudaMemcpyAsync(l0.data(), lens.p, l0.size() * 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  std::vector<DevNum> P(nleaf), Q(nleaf);
+  for (uint32_t j = 0; j < nleaf; j++) {
+    P[j] = {(uint32_t *)level.p + (size_t)(2 * j) * LEAF_STRIDE, l0[2 * j]};
+    Q[j] = {(uint32_t *)level.p + (size_t)(2 * j + 1) * LEAF_STRIDE, l0[2 * j + 1]};
+  }
+  while (P.size() > 1) {
+    const size_t c = P.size(), np = c / 2;
+    const bool odd = c & 1;
+    // layout of the next level: per pair t = P_l*Q_r, Q' = Q_l*Q_r, P' = t + P_r
+    std::vector<size_t> offT(np), offQ(np), offP(np), nT(np), nQ(np), nP(np);
+    size_t total = 0;
+    for (size_t i = 0; i < np; i++) {
+      nT[i] = P[2 * i].len + Q[2 * i + 1].len;
+      nQ[i] = Q[2 * i].len + Q[2 * i + 1].len;
+      nP[i] = std::max(nT[i], P[2 * i + 1].len) + 1;
+      offT[i] = total; total += (nT[i] + 63) & ~size_t(63);
+      offQ[i] = total; total += (nQ[i] + 63) & ~size_t(63);
+      offP[i] = total; total += (nP[i] + 63) & ~size_t(63);
+    }
+    size_t offOddP = total, offOddQ = total;
+    if (odd) {
+      offOddP = total; total += (P[c - 1].len + 63) & ~size_t(63);
+      offOddQ = total; total += (Q[c - 1].len + 63) & ~size_t(63);
+    }
+    DevBuf next;
+    if ((r = next.alloc(total * 4))) return r;
+    uint32_t *nb = (uint32_t *)next.p;
+    // products
+    std::vector<bc_mul_desc> md(2 * np);
+    for (size_t i = 0; i < np; i++) {
+      md[2 * i] = {nb + offT[i], nT[i], P[2 * i].p, P[2 * i].len, Q[2 * i + 1].p, Q[2 * i + 1].len};
+      md[2 * i + 1] = {nb + offQ[i], nQ[i], Q[2 * i].p, Q[2 * i].len, Q[2 * i + 1].p, Q[2 * i + 1].len};
+    }
+    if ((r = mul_batch_locked(md.data(), md.size(), st, nullptr, BC_BATCH_DEVICE_OPERANDS))) return r;
+    // significant lengths of the products, then the additions
+    std::vector<TrimDesc> td(2 * np);
+    for (size_t i = 0; i < 2 * np; i++) td[i] = {md[i].C, md[i].CL};
+    std::vector<AddDesc> ad(np);
+    unsigned long long tiles = 0;  // bound from the untrimmed lengths; sizes the status words
+    for (size_t i = 0; i < np; i++) {
+      const unsigned long long n = std::max<unsigned long long>(nT[i], P[2 * i + 1].len);
+      ad[i] = {nb + offT[i], P[2 * i + 1].p, nb + offP[i], nT[i], P[2 * i + 1].len, n, 0};
+      tiles += n / ADD_TILE + 1;
+    }
+    // scratch: trim descs, product lengths, add descs, status, counter+flags, add lengths
+    const size_t o_td = 0, o_tl = align256(o_td + td.size() * sizeof(TrimDesc));
+    const size_t o_ad = align256(o_tl + 2 * np * 8), o_st = align256(o_ad + np * sizeof(AddDesc));
+    const size_t o_ctr = align256(o_st + tiles * 4), o_al = o_ctr + 256, o_end = align256(o_al + np * 8);
+    DevBuf meta;
+    if ((r = meta.alloc(o_end))) return r;
+    char *mb = (char *)meta.p;
+    CK(cudaMemcpyAsync(mb + o_td, td.data(), td.size() * sizeof(TrimDesc), cudaMemcpyHostToDevice, g.stream));
+    k_trim<<<(unsigned)((2 * np + 255) / 256), 256, 0, g.stream>>>((const TrimDesc *)(mb + o_td), (uint32_t)(2 * np),
+                                                                 (unsigned long long *)(mb + o_tl));
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> tl(2 * np);
+    CK(cudaMemcpyAsync(tl.data(), mb + o_tl, tl.size() * 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    tiles = 0;
+    for (size_t i = 0; i < np; i++) {
+      ad[i].lx = tl[2 * i];
+      ad[i].n = std::max<unsigned long long>(ad[i].lx, ad[i].ly);
+      ad[i].tile0 = tiles;
+      tiles += ad[i].n / ADD_TILE + 1;
+    }
+    CK(cudaMemcpyAsync(mb + o_ad, ad.data(), ad.size() * sizeof(AddDesc), cudaMemcpyHostToDevice, g.stream));
+    CK(cudaMemsetAsync(mb + o_st, 0, o_al - o_st, g.stream));
+    AddParams ap;
+    ap.items = (const AddDesc *)(mb + o_ad);
+    ap.nitems = (int)np;
+    ap.tiles = tiles;
+    ap.counter = (unsigned int *)(mb + o_ctr);
+    ap.flags = (unsigned int *)(mb + o_ctr + 128);
+    ap.status = (uint32_t *)(mb + o_st);
+    ap.len = (unsigned long long *)(mb + o_al);
+    const unsigned grid = (unsigned)std::min<unsigned long long>(tiles, (unsigned long long)g.sm_count * 4);
+    k_add<<<grid, ADD_NT, 0, g.stream>>>(ap);
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> al(np);
+    unsigned int aflags = 0;
+    CK(cudaMemcpyAsync(al.data(), ap.len, np * 8, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(&aflags, ap.flags, 4, cudaMemcpyDeviceToHost, g.stream));
+    if (odd) {
+      CK(cudaMemcpyAsync(nb + offOddP, P[c - 1].p, P[c - 1].len * 4, cudaMemcpyDeviceToDevice, g.stream));
+      CK(cudaMemcpyAsync(nb + offOddQ, Q[c - 1].p, Q[c - 1].len * 4, cudaMemcpyDeviceToDevice, g.stream));
+    }
+    CK(cudaStreamSynchronize(g.stream));
+    if (aflags) return fail(BC_ERR_TIMEOUT);
+    std::vector<DevNum> P2(np + odd), Q2(np + odd);
+    for (size_t i = 0; i < np; i++) {
+      P2[i] = {nb + offP[i], (size_t)al[i]};
+      Q2[i] = {nb + offQ[i], (size_t)tl[2 * i + 1]};
+    }
+    if (odd) {
+      P2[np] = {nb + offOddP, P[c - 1].len};
+      Q2[np] = {nb + offOddQ, Q[c - 1].len};
+    }
+    P.swap(P2);
+    Q.swap(Q2);
+    std::swap(level.p, next.p);  // the old level is freed with `next`
+  }
+  hP.resize(P[0].len);
+  hQ.resize(Q[0].len);
+  CK(cudaMemcpyAsync(hP.data(), P[0].p, P[0].len * 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaMemcpyAsync(hQ.data(), Q[0].p, Q[0].len * 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
   return BC_OK;
 }
 
@@ -1188,6 +1335,28 @@ int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, b
   int r = mul_batch_locked(items, n, &st, nullptr, flags);
   if (stats) *stats = st;
   return r;
+}
+
+int bc_gpu_e_series(uint32_t a, uint32_t b, uint32_t **P, size_t *PL, uint32_t **Q, size_t *QL) {
+  if (!P || !PL || !Q || !QL) return BC_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  std::vector<uint32_t> hp, hq;
+  bc_batch_stats st{};
+  int r = e_series_locked(a, b, hp, hq, &st);
+  if (r) return r;
+  *P = (uint32_t *)malloc(std::max<size_t>(hp.size(), 1) * 4);
+  *Q = (uint32_t *)malloc(std::max<size_t>(hq.size(), 1) * 4);
+  if (!*P || !*Q) {
+    free(*P);
+    free(*Q);
+    *P = *Q = nullptr;
+    return fail(BC_ERR_NOMEM);
+  }
+  memcpy(*P, hp.data(), hp.size() * 4);
+  memcpy(*Q, hq.data(), hq.size() * 4);
+  *PL = hp.size();
+  *QL = hq.size();
+  return BC_OK;
 }
 
 int bc_gpu_set_stream(void *stream) {

@@ -29,6 +29,8 @@ typedef struct {
 void *bc_xmalloc(size_t n);
 void *bc_xrealloc(void *p, size_t n);
 void bc_mul_operands(const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p, bc_operand *oa, bc_operand *ob);
+/* Initialise the GPU engine once (aborts with a message if there is none). */
+void bc_host_ensure_gpu(void);
 /* All items on the GPU in one batch; aborts with a message on failure. */
 void bc_host_gpu_batch(bc_gpu_item *items, size_t n);
 /* Product of small operands on the host (schoolbook), CT may alias. */

@@ -11,7 +11,12 @@
  *   mode 1  level order: subtrees of at most LEAF_TERMS terms run the same
  *           recursion on host threads (all their products are below 100
  *           limbs, the reference's host range), and every level above them
- *           multiplies all of its 2*nodes products in one bigfloat_mul_batch.
+ *           multiplies all of its 2*nodes products in one bigfloat_mul_batch;
+ *   mode 2  the whole tree in device memory (bc_gpu_e_series): P and Q
+ *           cross to the host once, at the root.
+ * P and Q are the same integers in every mode (they do not depend on where
+ * ranges split) and come out exponent 0 with no top zero limbs, as the
+ * reference's products and additions leave them.
  */
 #include <math.h>
 #include <stdio.h>
@@ -19,6 +24,7 @@
 #include <string.h>
 #include <time.h>
 
+#include "bc_gpu.h"
 #include "bc_host.h"
 #include "bench.h"
 #include "bigfloat.h"
@@ -72,6 +78,24 @@ static double wall_s(void) {
   struct timespec t;
   clock_gettime(CLOCK_MONOTONIC, &t);
   return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+/* mode 2: the series on the GPU, the root's P and Q back as bigfloats. */
+static void bsr_device(bigfloat_t P, bigfloat_t Q, uint32_t a, uint32_t b) {
+  bc_host_ensure_gpu();
+  uint32_t *p = NULL, *q = NULL;
+  size_t pl = 0, ql = 0;
+  double t0 = wall_s();
+  int rc = bc_gpu_e_series(a, b, &p, &pl, &q, &ql);
+  if (rc != BC_OK) {
+    fprintf(stderr, "bluecrunch: binary splitting on the GPU failed: %s\n", bc_gpu_strerror(rc));
+    abort();
+  }
+  if (getenv("BC_STATS")) printf("    binary splitting on the GPU: %.3f s\n", wall_s() - t0);
+  free(P->coef);
+  P->coef = p; P->len = pl; P->exp = 0; P->sign = 1;
+  free(Q->coef);
+  Q->coef = q; Q->len = ql; Q->exp = 0; Q->sign = 1;
 }
 
 static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
@@ -199,7 +223,8 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   bigfloat_t P, Q;
   bigfloat_new(P);
   bigfloat_new(Q);
-  if (mode == 1) bsr_levels(P, Q, 0, (uint32_t)terms);
+  if (mode == 2) bsr_device(P, Q, 0, (uint32_t)terms);
+  else if (mode == 1) bsr_levels(P, Q, 0, (uint32_t)terms);
   else bsr(P, Q, 0, (uint32_t)terms);
   task_end(1);
 

@@ -1,8 +1,9 @@
-/* main.c — command line: bluecrunch <digits> [--per-call]
+/* main.c — command line: bluecrunch <digits> [--per-call | --levels]
  * Computes e to <digits> decimal digits into ./e.txt and ./e-hex.txt, like
- * the reference's main.c:169-219; products run on the GPU.  --per-call uses
- * the reference's recursion with one GPU product per call instead of the
- * level-batched tree. */
+ * the reference's main.c:169-219; products run on the GPU.  By default the
+ * binary-splitting tree lives in device memory; --levels keeps the tree on
+ * the host with each level's products in one GPU batch; --per-call uses the
+ * reference's recursion with one GPU product per call. */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -12,16 +13,19 @@
 
 int main(int argc, char *argv[]) {
   if (argc < 2) {
-    printf("Usage %s <number of digits> [--per-call] - Computes Eulers constant\n", argv[0]);
+    printf("Usage %s <number of digits> [--per-call | --levels] - Computes Eulers constant\n", argv[0]);
     return 0;
   }
   size_t digits = strtoull(argv[1], NULL, 10);
-  int mode = 1;
-  for (int i = 2; i < argc; i++)
+  int mode = 2;
+  for (int i = 2; i < argc; i++) {
     if (!strcmp(argv[i], "--per-call")) mode = 0;
+    if (!strcmp(argv[i], "--levels")) mode = 1;
+  }
+  static const char *names[] = {"one product per call", "tree levels batched", "tree in device memory"};
   printf("Configuration:\n");
   printf("Digits:           %zu\n", digits);
-  printf("Multiply:         B200 FP64 FFT (%s)\n", mode ? "tree levels batched" : "one product per call");
+  printf("Multiply:         B200 FP64 FFT (%s)\n", names[mode]);
   printf("Output File:      ./e.txt\n\n");
   task_start(0, "Starting calculation");
   int rc = bluecrunch_e(digits, mode, NULL);

@@ -74,7 +74,7 @@ static void init_once(void) {
   g_init_rc = bc_gpu_init(&cfg);
 }
 
-static void ensure_gpu(void) {
+void bc_host_ensure_gpu(void) {
   pthread_once(&g_once, init_once);
   if (g_init_rc != BC_OK) {
     fprintf(stderr, "bluecrunch: GPU engine unavailable: %s\n", bc_gpu_strerror(g_init_rc));
@@ -122,7 +122,7 @@ static void count(size_t products, size_t calls, double secs) {
 }
 
 int _fft_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *BT, size_t BL) {
-  ensure_gpu();
+  bc_host_ensure_gpu();
   bc_mul_stats st;
   double t0 = now_s();
   int rc = bc_gpu_mul(CT, CL, AT, AL, BT, BL, &st);
@@ -136,7 +136,7 @@ int _fft_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *BT, siz
 }
 
 void bc_host_gpu_batch(bc_gpu_item *items, size_t n) {
-  ensure_gpu();
+  bc_host_ensure_gpu();
   bc_mul_desc *d = (bc_mul_desc *)bc_xmalloc(n * sizeof(bc_mul_desc));
   for (size_t i = 0; i < n; i++) {
     d[i].C = items[i].C; d[i].CL = items[i].CL;

@@ -20,6 +20,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "bc_host.h"
 #include "bench.h"
@@ -252,7 +253,14 @@ typedef struct node {
   int child_h, child_l;    /* indices in the next level */
 } node;
 
+static double wall_now(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
 static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct *y0, size_t n0, size_t g) {
+  double t0 = wall_now(), t_split = 0, t_leaf = 0, t_merge = 0;
   node **lv = NULL;
   size_t *cnt = NULL;
   int nlv = 0;
@@ -314,6 +322,8 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
     cnt[nlv] = c;
     nlv++;
   }
+  t_split = wall_now() - t0;
+  t0 = wall_now();
   /* leaves, all levels at once, in parallel */
   for (int d = 0; d < nlv; d++) {
     node *L = lv[d];
@@ -326,6 +336,8 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
       convert_trunc(&x->s, &x->y, x->k, x->n);
     }
   }
+  t_leaf = wall_now() - t0;
+  t0 = wall_now();
   /* bottom-up merges, one level at a time, nodes of a level in parallel */
   for (int d = nlv - 2; d >= 0; d--) {
     node *L = lv[d], *N = lv[d + 1];
@@ -343,6 +355,10 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
     }
     free(N);
   }
+  t_merge = wall_now() - t0;
+  if (getenv("BC_STATS"))
+    printf("    conversion: %d levels, splits and products %.3f s, leaves %.3f s, merges %.3f s\n", nlv, t_split,
+           t_leaf, t_merge);
   /* hand the root's digits to the target */
   free(target->coef);
   *target = lv[0][0].s;
@@ -420,10 +436,26 @@ size_t bigfloat_to_string(char *string, const bigfloat_t value, size_t digits, i
   size_t min_c;
   size_t per = base == 10 ? 8 : 9;
   min_c = value->len > digits / per ? value->len - digits / per - 1 : 0;
-  while (c-- > min_c) {
-    string += base == 10 ? limb_dec(value->coef[c], string) : limb_hex(value->coef[c], string);
-    if ((size_t)(string - start) >= digits) break;
+  /* The reference's loop (string.c:93-111) emits limbs c-1, c-2, ... down to
+   * min_c, w characters each, and stops after the first limb that brings the
+   * string to `digits` characters.  Every limb's place is known in advance,
+   * so the limbs are written in parallel. */
+  const size_t w = base == 10 ? 9 : 8;
+  const size_t prefix = (size_t)(string - start);
+  const size_t avail = c > min_c ? c - min_c : 0;
+  size_t n = avail;
+  if (n) {
+    const size_t need = digits > prefix ? (digits - prefix + w - 1) / w : 1;
+    if (need < n) n = need;
   }
+  const long nn = (long)n;
+#pragma omp parallel for schedule(static) if (nn > 100000)
+  for (long k = 0; k < nn; k++) {
+    const uint32_t v = value->coef[c - 1 - (size_t)k];
+    if (base == 10) limb_dec(v, string + (size_t)k * w);
+    else limb_hex(v, string + (size_t)k * w);
+  }
+  string += n * w;
   *string++ = '\0';
   if ((size_t)(string - start) > digits) {
     start[digits + 1] = '\0';

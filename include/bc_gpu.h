@@ -99,10 +99,20 @@ int bc_gpu_mul(uint32_t *C, size_t CL, const uint32_t *A, size_t AL,
 int bc_gpu_mul_batch(const bc_mul_desc *items, size_t n, bc_batch_stats *stats);
 
 /* Same, with hints: BC_BATCH_HOST_OPERANDS declares every A, B and C to be
- * host memory (skips the per-pointer device query, which dominates batches
- * of millions of small products). */
-enum { BC_BATCH_HOST_OPERANDS = 1 };
+ * host memory, BC_BATCH_DEVICE_OPERANDS every one to be device memory (each
+ * skips the per-pointer memory query, which dominates batches of millions of
+ * small products). */
+enum { BC_BATCH_HOST_OPERANDS = 1, BC_BATCH_DEVICE_OPERANDS = 2 };
 int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, bc_batch_stats *stats);
+
+/* The binary-splitting sum of e's series on the GPU: P and Q with
+ * P/Q = sum_{j=a+1}^{b} 1/((a+1)(a+2)...j) and Q = (a+1)(a+2)...b, the
+ * integers the reference's e_BSR (main.c:63-109) builds on the host.  Every
+ * intermediate value stays in device memory (leaves of 64 terms, then one
+ * batched product level and one addition kernel per tree level).  On
+ * success *P and *Q are malloc'd host arrays of *PL and *QL little-endian
+ * limbs without top zeros (the caller frees them).  Needs b < 2^32 - 16. */
+int bc_gpu_e_series(uint32_t a, uint32_t b, uint32_t **P, size_t *PL, uint32_t **Q, size_t *QL);
 
 /* Launch on this CUDA stream (cudaStream_t as void*; NULL = library stream).
  * Calls still return only when their results are complete. */

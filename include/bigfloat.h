@@ -74,7 +74,8 @@ void bigfloat_mul_batch(bigfloat_mul_item *items, size_t n);
 /* e to `digits` decimal digits; writes "2." + digits into e.txt and the hex
  * expansion into e-hex.txt in `outdir` (NULL = current directory).  mode 0:
  * the reference's recursive binary splitting, one product per GPU call;
- * mode 1: tree levels batched (bigfloat_mul_batch). Returns 0 on success. */
+ * mode 1: tree levels batched (bigfloat_mul_batch); mode 2: the whole tree
+ * in device memory (bc_gpu_e_series). Returns 0 on success. */
 int bluecrunch_e(size_t digits, int mode, const char *outdir);
 
 /* Product counters since the last reset (for tests and benchmarks). */

@@ -15,9 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MD5 = json.load(open(os.path.join(HERE, "golden", "e_md5.json")))["published"]["digits_to_md5"]
 
 
-def _e(digits, per_call=False, env=None):
+def _e(digits, per_call=False, env=None, levels=False):
     with tempfile.TemporaryDirectory() as d:
-        cmd = [bc.CLI, str(digits)] + (["--per-call"] if per_call else [])
+        cmd = [bc.CLI, str(digits)] + (["--per-call"] if per_call else []) + (["--levels"] if levels else [])
         e = dict(os.environ, **(env or {}))
         res = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=900, env=e)
         assert res.returncode == 0, "bluecrunch %s failed (%d): %s" % (digits, res.returncode, res.stderr[-2000:])
@@ -29,8 +29,11 @@ def _e(digits, per_call=False, env=None):
 
 @pytest.mark.parametrize("digits", [1000, 10000, 100000, 1000000])
 def test_e_batched_matches_published_md5(digits):
-    md5, _, _ = _e(digits)
+    md5, _, _ = _e(digits)  # the splitting tree in device memory
     assert md5 == MD5[str(digits)]
+    if digits <= 100000:
+        md5, _, _ = _e(digits, levels=True)  # host tree, batched levels
+        assert md5 == MD5[str(digits)]
 
 
 def test_e_per_call_1e6_matches_batched():

@@ -17,7 +17,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _run_e(digits, tmp, per_call=False):
-    cmd = [bc.CLI, str(digits)] + (["--per-call"] if per_call else [])
+    # host tree (all products of these sizes stay on the host)
+    cmd = [bc.CLI, str(digits)] + (["--per-call"] if per_call else ["--levels"])
     subprocess.run(cmd, cwd=tmp, check=True, stdout=subprocess.DEVNULL, timeout=120)
     return open(os.path.join(tmp, "e.txt"), "rb").read(), open(os.path.join(tmp, "e-hex.txt"), "rb").read()
 
