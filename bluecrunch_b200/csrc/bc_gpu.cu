@@ -26,6 +26,7 @@
 #include "bc_gpu.h"
 #include "bc_pipe.cuh"
 #include "bc_bsr.cuh"
+#include "bc_radix.cuh"
 
 using namespace bc;
 
@@ -341,7 +342,12 @@ int ensure_tables(const Shape &s, Tables **out) {
   fill_tables(s, lay, host.data());
   double2 *dev = nullptr;
   CK(cudaMalloc(&dev, lay.total * sizeof(double2)));
-  CK(cudaMemcpy(dev, host.data(), lay.total * sizeof(double2), cudaMemcpyHostToDevice));
+  // On the library stream, then waited for: a plain cudaMemcpy from pageable
+  // memory returns once the data is staged, before the copy lands, and the
+  // legacy stream it uses does not order with the library's non-blocking
+  // stream, so the first kernels of a new length could read stale tables.
+  CK(cudaMemcpyAsync(dev, host.data(), lay.total * sizeof(double2), cudaMemcpyHostToDevice, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
   auto res = g.tables.emplace((size_t)s.M, tables_at(lay, dev));
   *out = &res.first->second;
   return BC_OK;
@@ -607,6 +613,14 @@ ClassParams class_params(const Shape &s, const Tables &tb) {
 }
 
 // ------------------------------------------------------------------ arena
+// $BC_POISON: fill fresh device scratch with 0xA5 bytes, so that a kernel
+// that reads scratch it has not written gives different results (a check
+// for the tests; off by default).
+bool poison_on() {
+  static const bool on = getenv("BC_POISON") != nullptr;
+  return on;
+}
+
 int arena_reserve(size_t bytes) {
   if (bytes <= g.arena_cap) return BC_OK;
   if (bytes > g.arena_limit) return fail(BC_ERR_NOMEM);
@@ -629,6 +643,7 @@ int arena_reserve(size_t bytes) {
     }
   }
   g.arena_cap = want;
+  if (poison_on()) CK(cudaMemsetAsync(g.arena, 0xA5, want, g.stream));  // ordered with the library stream
   return BC_OK;
 }
 
@@ -714,14 +729,26 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-// Pageable host operands and results go through pinned staging buffers: one
-// host-to-device and one device-to-host copy per batch instead of one per
-// item, filled and drained by par_copy.  Pinned host arrays copy directly.
-struct PinnedStage {
-  char *p = nullptr;
-  size_t cap = 0;
+// Pageable host operands and results cross through a ring of two pinned
+// chunks of kRingChunk bytes: the operands of a batch form one contiguous
+// span on the device, filled chunk by chunk (par_copy into one chunk while
+// the other's copy to the device runs), and the results leave the same way.
+// No per-item copies and no pinned allocation that grows with the batch.
+// Pinned host arrays copy directly.
+constexpr size_t kRingChunk = size_t(64) << 20;
+struct PinnedRing {
+  char *half[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool pending[2] = {false, false};
 };
-PinnedStage g_pin_in, g_pin_out;
+PinnedRing g_ring;
+
+// One array's place in a staged span: span offset, host address, bytes.
+struct SpanJob {
+  size_t off;
+  char *host;
+  size_t n;
+};
 
 // Host-side phase times of the batch path, printed at exit when $BC_PROFILE
 // is set (seconds).
@@ -755,15 +782,79 @@ struct PhaseTimer {
   ~PhaseTimer() { next(acc); }
 };
 
-int pinned_reserve(PinnedStage &ps, size_t bytes) {
-  if (bytes <= ps.cap) return BC_OK;
+int ring_ready() {
+  if (g_ring.half[0]) return BC_OK;
   PhaseTimer pt(&g_prof.pin_alloc);
-  if (ps.p) CK(cudaFreeHost(ps.p));
-  ps.p = nullptr;
-  ps.cap = 0;
-  size_t want = std::max(2 * bytes, (size_t)1 << 26);  // doubling: few reallocations
-  CK(cudaHostAlloc((void **)&ps.p, want, cudaHostAllocDefault));
-  ps.cap = want;
+  for (int h = 0; h < 2; h++) {
+    CK(cudaHostAlloc((void **)&g_ring.half[h], kRingChunk, cudaHostAllocDefault));
+    CK(cudaEventCreateWithFlags(&g_ring.ev[h], cudaEventDisableTiming));
+  }
+  return BC_OK;
+}
+
+// Pieces of the jobs (sorted by offset) inside span window [w0, w0 + len),
+// as copies between `chunk` (the window's pinned image) and the host arrays.
+// `j` walks the jobs across successive windows.
+void window_pieces(const std::vector<SpanJob> &jobs, size_t &j, size_t w0, size_t len, char *chunk, bool to_chunk,
+                   std::vector<CopyJob> &out) {
+  out.clear();
+  while (j < jobs.size() && jobs[j].off < w0 + len) {
+    const SpanJob &sj = jobs[j];
+    const size_t s0 = std::max(sj.off, w0), s1 = std::min(sj.off + sj.n, w0 + len);
+    if (s1 > s0) {
+      char *c = chunk + (s0 - w0), *h = sj.host + (s0 - sj.off);
+      out.push_back(to_chunk ? CopyJob{c, h, s1 - s0} : CopyJob{h, c, s1 - s0});
+    }
+    if (sj.off + sj.n <= w0 + len) j++;
+    else break;
+  }
+}
+
+// Host arrays -> device span [dev, dev + total) through the ring.
+int stage_h2d(char *dev, const std::vector<SpanJob> &jobs, size_t total) {
+  int r = ring_ready();
+  if (r) return r;
+  std::vector<CopyJob> pieces;
+  size_t j = 0;
+  for (size_t w0 = 0, c = 0; w0 < total; w0 += kRingChunk, c++) {
+    const int h = (int)(c & 1);
+    const size_t len = std::min(kRingChunk, total - w0);
+    if (g_ring.pending[h]) CK(cudaEventSynchronize(g_ring.ev[h]));
+    window_pieces(jobs, j, w0, len, g_ring.half[h], true, pieces);
+    par_copy(pieces);
+    CK(cudaMemcpyAsync(dev + w0, g_ring.half[h], len, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaEventRecord(g_ring.ev[h], g.stream));
+    g_ring.pending[h] = true;
+  }
+  return BC_OK;
+}
+
+// Device span [dev, dev + total) -> host arrays through the ring (the copy
+// of chunk c+1 runs while chunk c is drained).
+int stage_d2h(const char *dev, const std::vector<SpanJob> &jobs, size_t total) {
+  int r = ring_ready();
+  if (r) return r;
+  for (int h = 0; h < 2; h++)
+    if (g_ring.pending[h]) { CK(cudaEventSynchronize(g_ring.ev[h])); g_ring.pending[h] = false; }
+  const size_t nch = (total + kRingChunk - 1) / kRingChunk;
+  auto issue = [&](size_t c) -> int {
+    const int h = (int)(c & 1);
+    const size_t w0 = c * kRingChunk, len = std::min(kRingChunk, total - w0);
+    CK(cudaMemcpyAsync(g_ring.half[h], dev + w0, len, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaEventRecord(g_ring.ev[h], g.stream));
+    return BC_OK;
+  };
+  if (nch && (r = issue(0))) return r;
+  std::vector<CopyJob> pieces;
+  size_t j = 0;
+  for (size_t c = 0; c < nch; c++) {
+    if (c + 1 < nch && (r = issue(c + 1))) return r;
+    const int h = (int)(c & 1);
+    CK(cudaEventSynchronize(g_ring.ev[h]));
+    const size_t w0 = c * kRingChunk, len = std::min(kRingChunk, total - w0);
+    window_pieces(jobs, j, w0, len, g_ring.half[h], false, pieces);
+    par_copy(pieces);
+  }
   return BC_OK;
 }
 
@@ -773,7 +864,6 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   const bool all_host = flags_in & BC_BATCH_HOST_OPERANDS;
   const bool all_dev = flags_in & BC_BATCH_DEVICE_OPERANDS;
   const size_t nw = works.size();
-  double scratch = 0;
   PhaseTimer pt(&g_prof.layout);
   g_prof.items += nw;
   // ---- classes (M, square); items of a class get contiguous slabs
@@ -844,18 +934,14 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   // ---- inputs
   pt.next(&g_prof.copy_in);
   if (stage_in) {
-    pt.next(&scratch);
-    if ((r = pinned_reserve(g_pin_in, stage_in))) return r;
-    pt.next(&g_prof.copy_in);
-    std::vector<CopyJob> jobs;
+    std::vector<SpanJob> jobs;  // in increasing span offset
     jobs.reserve(2 * nw);
     for (size_t i = 0; i < nw; i++) {
       const bc_mul_desc &d = items[works[i]->idx];
-      if (pin_in_off[i] != SIZE_MAX) jobs.push_back({g_pin_in.p + pin_in_off[i], (const char *)d.A, works[i]->pl.AL * 4});
-      if (pin_inB_off[i] != SIZE_MAX) jobs.push_back({g_pin_in.p + pin_inB_off[i], (const char *)d.B, works[i]->pl.BL * 4});
+      if (pin_in_off[i] != SIZE_MAX) jobs.push_back({pin_in_off[i], (char *)d.A, works[i]->pl.AL * 4});
+      if (pin_inB_off[i] != SIZE_MAX) jobs.push_back({pin_inB_off[i], (char *)d.B, works[i]->pl.BL * 4});
     }
-    par_copy(jobs);
-    CK(cudaMemcpyAsync(base + off_stage_in, g_pin_in.p, stage_in, cudaMemcpyHostToDevice, g.stream));
+    if ((r = stage_h2d(base + off_stage_in, jobs, stage_in))) return r;
     st->h2d_bytes += stage_in;
     g_prof.bytes_in += stage_in;
   }
@@ -977,11 +1063,6 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     for (auto e : g.kev) cudaEventDestroy(e);
     g.kev.clear();
   }
-  if (stage_out) {
-    pt.next(&scratch);
-    if ((r = pinned_reserve(g_pin_out, stage_out))) return r;
-    pt.next(&g_prof.copy_out);
-  }
   bool copies = false, staged_out = false;
   std::vector<char> ok(nw);
   for (size_t i = 0; i < nw; i++) {
@@ -1006,19 +1087,16 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     }
   }
   if (staged_out) {
-    CK(cudaMemcpyAsync(g_pin_out.p, base + off_stage_out, stage_out, cudaMemcpyDeviceToHost, g.stream));
+    std::vector<SpanJob> jobs;  // in increasing span offset
+    jobs.reserve(nw);
+    for (size_t i = 0; i < nw; i++)
+      if (ok[i] && pin_out_off[i] != SIZE_MAX)
+        jobs.push_back({pin_out_off[i], (char *)items[works[i]->idx].C, items[works[i]->idx].CL * 4});
+    if ((r = stage_d2h(base + off_stage_out, jobs, stage_out))) return r;
     st->d2h_bytes += stage_out;
     g_prof.bytes_out += stage_out;
   }
   if (copies) CK(cudaStreamSynchronize(g.stream));
-  if (staged_out) {
-    std::vector<CopyJob> jobs;
-    jobs.reserve(nw);
-    for (size_t i = 0; i < nw; i++)
-      if (ok[i] && pin_out_off[i] != SIZE_MAX)
-        jobs.push_back({(char *)items[works[i]->idx].C, g_pin_out.p + pin_out_off[i], items[works[i]->idx].CL * 4});
-    par_copy(jobs);
-  }
   return BC_OK;
 }
 
@@ -1118,9 +1196,64 @@ struct DevBuf {  // cudaMalloc'd, freed on scope exit
   ~DevBuf() { if (p) cudaFree(p); }
   int alloc(size_t bytes) {
     CK(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+    if (poison_on()) CK(cudaMemsetAsync(p, 0xA5, std::max<size_t>(bytes, 256), g.stream));
     return BC_OK;
   }
 };
+
+// ------------------------------------------------------------------ radix conversion leaves
+// All leaves of one conversion in one launch: the fractions cross to the
+// device in one staged span, the digits come back in another.
+int radix_leaves_locked(const bc_radix_leaf *lv, size_t count, double alpha) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (count == 0) return BC_OK;
+  if (!lv) return fail(BC_ERR_INVALID);
+  std::vector<size_t> in_off(count), out_off(count);
+  size_t in_bytes = 0, out_bytes = 0;
+  for (size_t i = 0; i < count; i++) {
+    const bc_radix_leaf &l = lv[i];
+    if ((l.len && !l.y) || (l.k && !l.s)) return fail(BC_ERR_INVALID);
+    if (l.len + 1 > (size_t)RADIX_WINDOW || l.n + 1 > (size_t)RADIX_WINDOW || l.n > l.len + 1 ||
+        l.k > 0xffffffffu)
+      return fail(BC_ERR_TOO_LARGE);
+    in_off[i] = in_bytes;
+    in_bytes += align256(l.len * 4);
+    out_off[i] = out_bytes;
+    out_bytes += align256(l.k * 4);
+  }
+  const size_t o_desc = 0, o_in = align256(count * sizeof(RadixLeaf)), o_out = o_in + in_bytes,
+               o_flag = o_out + out_bytes, total = o_flag + 256;
+  int r = arena_reserve(total);
+  if (r) return r;
+  char *base = g.arena;
+  std::vector<SpanJob> jobs;
+  jobs.reserve(count);
+  std::vector<RadixLeaf> d(count);
+  for (size_t i = 0; i < count; i++) {
+    const bc_radix_leaf &l = lv[i];
+    if (l.len) jobs.push_back({in_off[i], (char *)l.y, l.len * 4});
+    d[i] = {(const uint32_t *)(base + o_in + in_off[i]), (uint32_t *)(base + o_out + out_off[i]), (uint32_t)l.len,
+            (uint32_t)l.n, (uint32_t)l.k, 0u};
+  }
+  if ((r = stage_h2d(base + o_in, jobs, in_bytes))) return r;
+  CK(cudaMemcpyAsync(base + o_desc, d.data(), count * sizeof(RadixLeaf), cudaMemcpyHostToDevice, g.stream));
+  CK(cudaMemsetAsync(base + o_flag, 0, 256, g.stream));
+  const unsigned grid =
+      (unsigned)std::min<size_t>((count + RADIX_WARPS - 1) / RADIX_WARPS, (size_t)g.sm_count * 16);
+  k_radix_leaves<<<grid, 32 * RADIX_WARPS, 0, g.stream>>>((const RadixLeaf *)(base + o_desc), (int)count, alpha,
+                                                          (unsigned *)(base + o_flag));
+  CK(cudaGetLastError());
+  unsigned flag = 0;
+  CK(cudaMemcpyAsync(&flag, base + o_flag, 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  if (flag) return fail(BC_ERR_TOO_LARGE);
+  jobs.clear();
+  for (size_t i = 0; i < count; i++)
+    if (lv[i].k) jobs.push_back({out_off[i], (char *)lv[i].s, lv[i].k * 4});
+  if ((r = stage_d2h(base + o_out, jobs, out_bytes))) return r;
+  CK(cudaStreamSynchronize(g.stream));
+  return BC_OK;
+}
 
 int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vector<uint32_t> &hQ,
                     bc_batch_stats *st) {
@@ -1357,6 +1490,11 @@ int bc_gpu_e_series(uint32_t a, uint32_t b, uint32_t **P, size_t *PL, uint32_t *
   *PL = hp.size();
   *QL = hq.size();
   return BC_OK;
+}
+
+int bc_gpu_radix_leaves(const bc_radix_leaf *leaves, size_t count, double alpha) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return radix_leaves_locked(leaves, count, alpha);
 }
 
 int bc_gpu_set_stream(void *stream) {

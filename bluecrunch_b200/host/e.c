@@ -228,12 +228,19 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   else bsr(P, Q, 0, (uint32_t)terms);
   task_end(1);
 
+  const int stats = getenv("BC_STATS") != NULL;
+  if (stats)
+    printf("    P: %zu limbs, top %08x; Q: %zu limbs, top %08x\n", P->len, P->len ? P->coef[P->len - 1] : 0,
+           Q->len, Q->len ? Q->coef[Q->len - 1] : 0);
   task_start(1, "Dividing");
   bigfloat_t one, tmp;
   bigfloat_new(one);
   bigfloat_set(one, 1);
   bigfloat_new(tmp);
   bigfloat_div(tmp, P, Q, p);
+  if (stats)
+    printf("    P/Q: %zu limbs, exp %lld, top %08x\n", tmp->len, (long long)tmp->exp,
+           tmp->len ? tmp->coef[tmp->len - 1] : 0);
   bigfloat_free(Q);
   bigfloat_add(P, tmp, one, p);
   bigfloat_free(tmp);

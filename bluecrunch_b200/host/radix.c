@@ -11,10 +11,10 @@
  *
  * Two drivers: convert_rec_percall() recurses like the reference (one GPU
  * product per node); convert_levels() walks the same tree level by level,
- * multiplies a whole level in one bigfloat_mul_batch, converts all leaves in
- * parallel on the host and combines each level in parallel.  Both produce
- * the same digits; bigfloat_radix uses the level driver unless
- * BC_RADIX_PERCALL is set.
+ * multiplies a whole level in one bigfloat_mul_batch, converts all leaves on
+ * the GPU in one launch (bc_gpu_radix_leaves) and combines each level in
+ * parallel on the host.  Both produce the same digits; bigfloat_radix uses
+ * the level driver unless BC_RADIX_PERCALL is set.
  */
 #include <math.h>
 #include <stdio.h>
@@ -22,6 +22,7 @@
 #include <string.h>
 #include <time.h>
 
+#include "bc_gpu.h"
 #include "bc_host.h"
 #include "bench.h"
 #include "bigfloat.h"
@@ -324,17 +325,34 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
   }
   t_split = wall_now() - t0;
   t0 = wall_now();
-  /* leaves, all levels at once, in parallel */
-  for (int d = 0; d < nlv; d++) {
-    node *L = lv[d];
-    long m = (long)cnt[d];
-#pragma omp parallel for schedule(dynamic, 4)
-    for (long i = 0; i < m; i++) {
-      node *x = &L[i];
-      if (x->k > KT) continue;
-      bigfloat_alloc(&x->s, x->k);
-      convert_trunc(&x->s, &x->y, x->k, x->n);
+  /* leaves, all levels at once, in one GPU launch (convert_trunc's rounds
+   * per leaf, bc_gpu_radix_leaves) */
+  {
+    size_t nleaf = 0;
+    for (int d = 0; d < nlv; d++)
+      for (size_t i = 0; i < cnt[d]; i++) nleaf += lv[d][i].k <= KT;
+    bc_radix_leaf *rl = (bc_radix_leaf *)bc_xmalloc((nleaf ? nleaf : 1) * sizeof(bc_radix_leaf));
+    size_t q = 0;
+    for (int d = 0; d < nlv; d++)
+      for (size_t i = 0; i < cnt[d]; i++) {
+        node *x = &lv[d][i];
+        if (x->k > KT) continue;
+        bigfloat_alloc(&x->s, x->k);
+        x->s.len = x->k;
+        rl[q].y = x->y.coef;
+        rl[q].len = x->y.len;
+        rl[q].n = x->n;
+        rl[q].k = x->k;
+        rl[q].s = x->s.coef;
+        q++;
+      }
+    bc_host_ensure_gpu();
+    int rc = bc_gpu_radix_leaves(rl, q, ALPHA);
+    if (rc != BC_OK) {
+      fprintf(stderr, "bigfloat_radix: GPU conversion of %zu leaves failed: %s\n", q, bc_gpu_strerror(rc));
+      abort();
     }
+    free(rl);
   }
   t_leaf = wall_now() - t0;
   t0 = wall_now();

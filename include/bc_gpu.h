@@ -114,6 +114,22 @@ int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, b
  * limbs without top zeros (the caller frees them).  Needs b < 2^32 - 16. */
 int bc_gpu_e_series(uint32_t a, uint32_t b, uint32_t **P, size_t *PL, uint32_t **Q, size_t *QL);
 
+/* Leaves of the binary-to-decimal conversion (the reference's
+ * convert_trunc, bigfloat/radix.c:41-91), all in one GPU launch: for each
+ * leaf, k base-10^9 digits of the fraction y (len host limbs below the
+ * point, n the limb count the digit positions refer to) into s[0..k), most
+ * significant last.  alpha is the caller's log(10^9)/log(2^32), so that
+ * every truncation point matches the caller's own arithmetic.  len + 1 and
+ * n + 1 must not exceed 1024 limbs (leaves of up to 1000 digits). */
+typedef struct {
+  const uint32_t *y;
+  size_t len;
+  size_t n;
+  size_t k;
+  uint32_t *s;
+} bc_radix_leaf;
+int bc_gpu_radix_leaves(const bc_radix_leaf *leaves, size_t count, double alpha);
+
 /* Launch on this CUDA stream (cudaStream_t as void*; NULL = library stream).
  * Calls still return only when their results are complete. */
 int bc_gpu_set_stream(void *stream);

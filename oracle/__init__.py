@@ -201,6 +201,32 @@ def reference(kind="serial"):
     return _cache[key]
 
 
+def convert_trunc(y, n, k, alpha):
+    """k base-10^9 digits of the fraction y (uint32 limbs below the point) by
+    the reference's convert_trunc rounds (bigfloat/radix.c:41-91): multiply
+    the window by 10^9 (its top limb cleared first, the carry out dropped),
+    take limb n - floor(alpha*(i-1)) of the window, then slide the window up
+    by floor(alpha*i) - floor(alpha*(i-1)) limbs.  Pure Python: small cases."""
+    import math
+    t = [int(v) for v in y] + [0]
+    base, tl = 0, len(t)
+    s = [0] * k
+    for i in range(1, k + 1):
+        t[base + tl - 1] = 0
+        c = 0
+        for j in range(base, base + tl):
+            v = t[j] * 1000000000 + c
+            t[j] = v & 0xFFFFFFFF
+            c = v >> 32
+        ni_1 = int(float(n) - math.floor(alpha * float(i - 1)))
+        ni = int(float(n) - math.floor(alpha * float(i)))
+        s[k - i] = t[base + ni_1]
+        base += ni_1 - ni
+        tl = ni + 1
+        t[base + tl - 1] = 0
+    return np.array(s, dtype=np.uint32)
+
+
 def splitmix64(seed, n):
     """SplitMix64 stream as uint64 (the synthetic-operand generator)."""
     out = np.empty(n, dtype=np.uint64)

@@ -114,3 +114,19 @@ def test_device_pointers_and_aliasing(gpu, orc):
     buf[:50000] = da
     gpu.mul(buf[:50000], db, CL=90000, out=buf)
     assert np.array_equal(buf.cpu().numpy().view(np.uint32), want)
+
+
+def test_batch_spanning_several_staging_chunks(gpu, orc):
+    """Pageable operands and results of one batch crossing in 64 MiB chunks:
+    items larger than a chunk, items straddling chunk boundaries, small ones
+    between them; each product checked modulo primes (sizes beyond the NTT's
+    few-second range)."""
+    sizes = [(9_000_000, 8_000_000), (300, 200), (17_000_000, 5_000_000), (1, 1), (4_000_000, 4_000_001),
+             (2_500, 70_000)]
+    items = [(limbs(500 + i, al), limbs(600 + i, bl), None) for i, (al, bl) in enumerate(sizes)]
+    outs, st = gpu.mul_batch(items, want_stats=True)
+    for (a, b, _), c in zip(items, outs):
+        assert len(c) == len(a) + len(b)
+        assert orc.modcheck(c, a, b, 4)
+    small = items[1]
+    assert np.array_equal(outs[1], exact(small[0], small[1], len(small[0]) + len(small[1])))

@@ -17,9 +17,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _run_e(digits, tmp, per_call=False):
-    # host tree (all products of these sizes stay on the host)
+    # host tree and the reference's recursive conversion: at these sizes every
+    # product and the conversion's single leaf stay on the host
     cmd = [bc.CLI, str(digits)] + (["--per-call"] if per_call else ["--levels"])
-    subprocess.run(cmd, cwd=tmp, check=True, stdout=subprocess.DEVNULL, timeout=120)
+    env = dict(os.environ, BC_RADIX_PERCALL="1")
+    subprocess.run(cmd, cwd=tmp, check=True, stdout=subprocess.DEVNULL, timeout=120, env=env)
     return open(os.path.join(tmp, "e.txt"), "rb").read(), open(os.path.join(tmp, "e-hex.txt"), "rb").read()
 
 

@@ -113,3 +113,30 @@ def test_reference_small_multiply_bug_documented():
                        b.ctypes.data_as(u32p), b.size)
     ti = lambda x: int.from_bytes(x.astype("<u4").tobytes(), "little")
     assert ti(c) - ti(a) * ti(b) == 1 << case["wrong_by_bit"]
+
+
+def test_convert_trunc_restatement_matches_reference():
+    """oracle.convert_trunc against the reference's own convert_trunc
+    (bigfloat/radix.c:41-91) from the compiled reference library."""
+    import ctypes
+    import math
+    if not oracle.have_reference("serial"):
+        pytest.skip("reference build not present")
+    from bluecrunch_b200.bigfloat import BF, Lib, limbs as bf_limbs
+    lib = Lib(oracle.reference_path("serial"))
+    fn = lib.dll.convert_trunc
+    fn.restype = None
+    fn.argtypes = [ctypes.POINTER(BF), ctypes.POINTER(BF), ctypes.c_size_t, ctypes.c_size_t]
+    alpha = math.log(1e9) / math.log(4294967296.0)
+    rng = np.random.default_rng(11)
+    for i in range(25):
+        k = int(rng.integers(1, 300))
+        n = int(math.floor((k * math.log(1e9) + math.log(4.0) + math.log(1000.0)) / math.log(4294967296.0) + 1))
+        ln = n + int(rng.integers(0, 2))
+        y = oracle.random_limbs(40 + i, ln)
+        yb = lib.make(y, exp=-n)
+        s = lib.make(np.zeros(k, dtype=np.uint32))
+        fn(s, yb, k, n)
+        assert np.array_equal(bf_limbs(s), oracle.convert_trunc(y, n, k, alpha)), (ln, n, k)
+        lib.free(yb)
+        lib.free(s)
