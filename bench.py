@@ -289,6 +289,39 @@ def run_batched(bc, torch, stream, n=8192, sibling=False, per_call=True, reps=2)
 
 
 # ---------------------------------------------------------------- GPU arm
+def run_e(digits, extra=()):
+    """e to `digits` decimal digits through the CLI (the reference's main.c
+    flow: binary splitting, Newton division, radix conversion, output files),
+    wall time of the whole process and the md5 of e.txt against the
+    published value (md5sums.txt of the reference)."""
+    import hashlib
+    import tempfile
+    cli = os.path.join(ROOT, "bluecrunch_b200", "bluecrunch")
+    pub = json.load(open(os.path.join(ROOT, "tests", "golden", "e_md5.json")))["published"]["digits_to_md5"]
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        res = subprocess.run([cli, str(digits), *extra], cwd=d, capture_output=True, text=True, timeout=1800)
+        wall = time.perf_counter() - t0
+        if res.returncode != 0:
+            return {"digits": digits, "mode": " ".join(extra) or "default", "error": res.stderr[-300:]}
+        h = hashlib.md5()
+        with open(os.path.join(d, "e.txt"), "rb") as f:
+            for blk in iter(lambda: f.read(1 << 24), b""):
+                h.update(blk)
+    phases = {}
+    for ln in res.stdout.splitlines():
+        ln = ln.strip()
+        for name in ("Summing", "Dividing", "Writing hex digits", "Converting to decimal", "Writing decimal digits"):
+            if ln.startswith(name) and "[" in ln:
+                try:
+                    phases[name] = float(ln.rsplit("[", 1)[1].split()[0])
+                except ValueError:
+                    pass
+    md5 = h.hexdigest()
+    return {"digits": digits, "mode": " ".join(extra) or "tree in device memory", "wall_s": round(wall, 3),
+            "phases_s": phases, "md5": md5, "md5_matches_published": pub.get(str(digits)) == md5}
+
+
 def gpu_arm(args):
     import torch
     import bluecrunch_b200 as bc
@@ -448,6 +481,14 @@ def gpu_arm(args):
             except Exception as exc:
                 batched.append({"sibling": sib, "error": str(exc)[:300]})
 
+    # ---- e to N digits end to end (CLI), default mode and, smaller, per call
+    e_runs = []
+    if rank == 0 and args.e_digits:
+        e_runs.append(run_e(args.e_digits))
+        if args.e_per_call:
+            e_runs.append(run_e(args.e_per_call, ("--per-call",)))
+            e_runs.append(run_e(args.e_per_call))
+
     # ---- CPU baseline: the reference multiply on the host cores, bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -488,6 +529,7 @@ def gpu_arm(args):
             "clocks": clk.summary(),
             "sweep": sweep,
             "batched": batched,
+            "e": e_runs,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -506,6 +548,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-items", type=int, default=8192)
+    ap.add_argument("--e-digits", type=int, default=100000000, help="e to this many digits (0: skip)")
+    ap.add_argument("--e-per-call", type=int, default=0,
+                    help="also e to this many digits with one GPU product per call, and in the default mode")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

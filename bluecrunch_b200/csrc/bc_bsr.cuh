@@ -4,9 +4,10 @@
 // and Q = (a+1)(a+2)..b by recursion on the host (main.c:63-109): leaves
 // P = 1, Q = b, and P = P0*Q1 + P1, Q = Q0*Q1 at each node.  These integers
 // do not depend on where the range is split, so the device version uses its
-// own tree: leaves of up to LEAF_TERMS consecutive terms computed one per
-// thread, then levels that pair neighbouring nodes, with both products of a
-// level in one batched FFT multiply and the additions in k_add below.
+// own tree: leaves of up to 1024 consecutive terms computed one per warp
+// (P(a,k+1) = P(a,k)*(k+1) + 1, Q(a,k+1) = Q(a,k)*(k+1)), then levels that
+// pair neighbouring nodes, with both products of a level in one batched FFT
+// multiply and the additions in k_add below.
 #pragma once
 #include <cuda/atomic>
 
@@ -14,49 +15,92 @@
 
 namespace bc {
 
-constexpr int LEAF_TERMS = 64;
-constexpr int LEAF_STRIDE = 66;  // limbs per leaf value: Q < 2^(32*64), P < 2Q
-constexpr int LEAF_NT = 64;  // 2 x 66 limbs x 64 threads = 33 KB of static shared memory
+// Wide leaves, one warp each: up to WLEAF_CAP limbs per value, lane l holding
+// limbs [32l, 32l+32) in registers.  Per term k both values are multiplied
+// by k (P also gets +1 at limb 0) lane by lane, and the carry out of a lane
+// enters the next one (a second carry past a full lane ripples, bounded by
+// 32 rounds).  A carry out of the top lane means the leaf was too wide for
+// the capacity: flagged, never written past the buffer.
+constexpr int WLEAF_LPL = 32;                    // limbs per lane
+constexpr int WLEAF_CAP = 32 * WLEAF_LPL;        // limbs per value
+constexpr int WLEAF_STRIDE = WLEAF_CAP + 2;      // limbs per stored value
+constexpr int WLEAF_WARPS = 4;                   // warps per CTA
 
-// Leaf j covers terms (a + j*LEAF_TERMS, min(b, a + (j+1)*LEAF_TERMS)]:
-// P = 1, Q = a0+1 for the first term, then P = P*k + 1, Q = Q*k for each
-// further k (P(a,k+1) = P(a,k)*Q(k,k+1) + P(k,k+1)).  Limbs live in shared
-// memory, limb i of thread t at i*LEAF_NT + t (no bank conflicts); outputs
-// go to out + (2j)*LEAF_STRIDE (P) and out + (2j+1)*LEAF_STRIDE (Q), lengths
-// to len[2j], len[2j+1].
-__global__ void __launch_bounds__(LEAF_NT) k_bsr_leaves(uint32_t a, uint32_t b, uint32_t nleaf, uint32_t *out,
-                                                        uint32_t *len) {
-  __shared__ uint32_t sP[LEAF_STRIDE * LEAF_NT], sQ[LEAF_STRIDE * LEAF_NT];
-  const int t = threadIdx.x;
-  const uint32_t j = blockIdx.x * LEAF_NT + t;
-  if (j >= nleaf) return;
-  const uint32_t a0 = a + j * (uint32_t)LEAF_TERMS;
-  const uint32_t b0 = min(b, a0 + (uint32_t)LEAF_TERMS);
-  uint32_t *P = sP + t, *Q = sQ + t;  // element i at [i * LEAF_NT]
-  int lp = 1, lq = 1;
-  P[0] = 1;
-  Q[0] = a0 + 1;
-  for (uint32_t k = a0 + 2; k <= b0; k++) {
-    unsigned long long c = 1;  // P*k + 1
-    for (int i = 0; i < lp; i++) {
-      const unsigned long long v = (unsigned long long)P[i * LEAF_NT] * k + c;
-      P[i * LEAF_NT] = (uint32_t)v;
-      c = v >> 32;
-    }
-    if (c) P[(lp++) * LEAF_NT] = (uint32_t)c;
-    c = 0;  // Q*k
-    for (int i = 0; i < lq; i++) {
-      const unsigned long long v = (unsigned long long)Q[i * LEAF_NT] * k + c;
-      Q[i * LEAF_NT] = (uint32_t)v;
-      c = v >> 32;
-    }
-    if (c) Q[(lq++) * LEAF_NT] = (uint32_t)c;
+// x = x*k + add0 across the warp; returns 1 if a carry left the top lane.
+__device__ __forceinline__ unsigned warp_mul_small(uint32_t (&x)[WLEAF_LPL], uint32_t k, uint32_t add0, int lane) {
+  unsigned overflow = 0;
+  uint32_t c = lane == 0 ? add0 : 0u;
+#pragma unroll
+  for (int q = 0; q < WLEAF_LPL; q++) {
+    const unsigned long long v = (unsigned long long)x[q] * k + c;
+    x[q] = (uint32_t)v;
+    c = (uint32_t)(v >> 32);
   }
-  uint32_t *oP = out + (size_t)(2 * j) * LEAF_STRIDE, *oQ = oP + LEAF_STRIDE;
-  for (int i = 0; i < lp; i++) oP[i] = P[i * LEAF_NT];
-  for (int i = 0; i < lq; i++) oQ[i] = Q[i * LEAF_NT];
-  len[2 * j] = (uint32_t)lp;
-  len[2 * j + 1] = (uint32_t)lq;
+  uint32_t out = c;
+  for (int round = 0; round < 32; round++) {
+    if (lane == 31 && out) overflow = 1u;
+    uint32_t cin = __shfl_up_sync(~0u, lane == 31 ? 0u : out, 1);
+    if (lane == 0) cin = 0;
+    if (!__any_sync(~0u, cin != 0)) break;
+    uint32_t t = cin;
+#pragma unroll
+    for (int q = 0; q < WLEAF_LPL; q++) {
+      const unsigned long long v = (unsigned long long)x[q] + t;
+      x[q] = (uint32_t)v;
+      t = (uint32_t)(v >> 32);
+    }
+    out = t;
+  }
+  return overflow;
+}
+
+// Leaf j covers terms (a + j*T, min(b, a + (j+1)*T)]; values go to
+// out + (2j)*WLEAF_STRIDE (P) and out + (2j+1)*WLEAF_STRIDE (Q), lengths to
+// len[2j], len[2j+1]; flags bit 0 on a capacity overflow.
+__global__ void __launch_bounds__(32 * WLEAF_WARPS) k_bsr_leaves_wide(uint32_t a, uint32_t b, uint32_t T,
+                                                                     uint32_t nleaf, uint32_t *out, uint32_t *len,
+                                                                     unsigned *flags) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t j = blockIdx.x * WLEAF_WARPS + (threadIdx.x >> 5);
+  if (j >= nleaf) return;  // whole warps leave together
+  const uint32_t a0 = a + j * T;
+  const uint32_t b0 = min(b, a0 + T);
+  uint32_t P[WLEAF_LPL], Q[WLEAF_LPL];
+#pragma unroll
+  for (int q = 0; q < WLEAF_LPL; q++) P[q] = Q[q] = 0;
+  if (lane == 0) {
+    P[0] = 1;
+    Q[0] = a0 + 1;
+  }
+  unsigned ovf = 0;
+  for (uint32_t k = a0 + 2; k <= b0; k++) {
+    ovf |= warp_mul_small(P, k, 1u, lane);
+    ovf |= warp_mul_small(Q, k, 0u, lane);
+  }
+  // lengths: highest nonzero limb + 1
+  int hp = -1, hq = -1;
+#pragma unroll
+  for (int q = 0; q < WLEAF_LPL; q++) {
+    if (P[q]) hp = lane * WLEAF_LPL + q;
+    if (Q[q]) hq = lane * WLEAF_LPL + q;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    hp = max(hp, __shfl_xor_sync(~0u, hp, o));
+    hq = max(hq, __shfl_xor_sync(~0u, hq, o));
+  }
+  uint32_t *oP = out + (size_t)(2 * j) * WLEAF_STRIDE, *oQ = oP + WLEAF_STRIDE;
+#pragma unroll
+  for (int q = 0; q < WLEAF_LPL; q++) {
+    const int i = lane * WLEAF_LPL + q;
+    if (i <= hp) oP[i] = P[q];
+    if (i <= hq) oQ[i] = Q[q];
+  }
+  if (lane == 0) {
+    len[2 * j] = (uint32_t)(hp + 1);
+    len[2 * j + 1] = (uint32_t)(hq + 1);
+  }
+  if (__any_sync(~0u, ovf != 0) && lane == 0) atomicOr(flags, 1u);
 }
 
 // Significant length of each product C_i of CL_i limbs whose operands had

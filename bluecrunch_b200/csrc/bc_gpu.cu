@@ -1259,20 +1259,37 @@ int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vect
                     bc_batch_stats *st) {
   if (!g.init) return fail(BC_ERR_NOT_INIT);
   if (b <= a || b > 0xfffffff0u) return fail(BC_ERR_INVALID);
-  const uint32_t nleaf = (b - a + LEAF_TERMS - 1) / LEAF_TERMS;
+  // leaves as wide as a warp holds: T terms give at most T*bits(b)/32 + 1
+  // limbs per value, which must stay within WLEAF_CAP
+  int bits = 0;
+  while (bits < 32 && (b >> bits)) bits++;
+  const uint32_t T = (uint32_t)std::min<long long>(1024, (long long)(WLEAF_CAP - 2) * 32 / bits);
+  const uint32_t nleaf = (b - a + T - 1) / T;
   DevBuf level, lens;
   int r;
-  if ((r = level.alloc((size_t)nleaf * 2 * LEAF_STRIDE * 4)) || (r = lens.alloc((size_t)nleaf * 2 * 4))) return r;
-  k_bsr_leaves<<<(nleaf + LEAF_NT - 1) / LEAF_NT, LEAF_NT, 0, g.stream>>>(a, b, nleaf, (uint32_t *)level.p,
-                                                                        (uint32_t *)lens.p);
+  if ((r = level.alloc((size_t)nleaf * 2 * WLEAF_STRIDE * 4)) || (r = lens.alloc((size_t)nleaf * 2 * 4 + 256)))
+    return r;
+  unsigned *lflags = (unsigned *)((char *)lens.p + (size_t)nleaf * 2 * 4);
+  CK(cudaMemsetAsync(lflags, 0, 4, g.stream));
+  k_bsr_leaves_wide<<<(nleaf + WLEAF_WARPS - 1) / WLEAF_WARPS, 32 * WLEAF_WARPS, 0, g.stream>>>(
+      a, b, T, nleaf, (uint32_t *)level.p, (uint32_t *)lens.p, lflags);
   CK(cudaGetLastError());
   std::vector<uint32_t> l0(2 * (size_t)nleaf);
+  unsigned leaf_overflow = 0;
   CK(cudaMemcpyAsync(l0.data(), lens.p, l0.size() * 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaMemcpyAsync(&leaf_overflow, lflags, 4, cudaMemcpyDeviceToHost, g.stream));
   CK(cudaStreamSynchronize(g.stream));
+  if (leaf_overflow) return fail(BC_ERR_TOO_LARGE);
+  const bool stats = getenv("BC_STATS") != nullptr;
+  double t_mul = 0, t_add = 0;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto secs = [](std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  };
   std::vector<DevNum> P(nleaf), Q(nleaf);
   for (uint32_t j = 0; j < nleaf; j++) {
-    P[j] = {(uint32_t *)level.p + (size_t)(2 * j) * LEAF_STRIDE, l0[2 * j]};
-    Q[j] = {(uint32_t *)level.p + (size_t)(2 * j + 1) * LEAF_STRIDE, l0[2 * j + 1]};
+    P[j] = {(uint32_t *)level.p + (size_t)(2 * j) * WLEAF_STRIDE, l0[2 * j]};
+    Q[j] = {(uint32_t *)level.p + (size_t)(2 * j + 1) * WLEAF_STRIDE, l0[2 * j + 1]};
   }
   while (P.size() > 1) {
     const size_t c = P.size(), np = c / 2;
@@ -1302,7 +1319,11 @@ int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vect
       md[2 * i] = {nb + offT[i], nT[i], P[2 * i].p, P[2 * i].len, Q[2 * i + 1].p, Q[2 * i + 1].len};
       md[2 * i + 1] = {nb + offQ[i], nQ[i], Q[2 * i].p, Q[2 * i].len, Q[2 * i + 1].p, Q[2 * i + 1].len};
     }
+    auto tl0 = now();
     if ((r = mul_batch_locked(md.data(), md.size(), st, nullptr, BC_BATCH_DEVICE_OPERANDS))) return r;
+    const double dm = secs(tl0);
+    t_mul += dm;
+    tl0 = now();
     // significant lengths of the products, then the additions
     std::vector<TrimDesc> td(2 * np);
     for (size_t i = 0; i < 2 * np; i++) td[i] = {md[i].C, md[i].CL};
@@ -1357,6 +1378,10 @@ int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vect
     }
     CK(cudaStreamSynchronize(g.stream));
     if (aflags) return fail(BC_ERR_TIMEOUT);
+    const double da = secs(tl0);
+    t_add += da;
+    if (stats && (dm + da > 0.05 || np < 4))
+      fprintf(stderr, "      series level: %zu nodes, products %.3f s, lengths and sums %.3f s\n", np, dm, da);
     std::vector<DevNum> P2(np + odd), Q2(np + odd);
     for (size_t i = 0; i < np; i++) {
       P2[i] = {nb + offP[i], (size_t)al[i]};
@@ -1370,6 +1395,7 @@ int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vect
     Q.swap(Q2);
     std::swap(level.p, next.p);  // the old level is freed with `next`
   }
+  if (stats) fprintf(stderr, "      series: %u leaves, products %.3f s, lengths and sums %.3f s\n", nleaf, t_mul, t_add);
   hP.resize(P[0].len);
   hQ.resize(Q[0].len);
   CK(cudaMemcpyAsync(hP.data(), P[0].p, P[0].len * 4, cudaMemcpyDeviceToHost, g.stream));

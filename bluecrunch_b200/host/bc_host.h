@@ -27,6 +27,9 @@ typedef struct {
 } bc_gpu_item;
 
 void *bc_xmalloc(size_t n);
+/* memcpy / memset to zero, split over the OpenMP threads when large. */
+void bc_par_memcpy(void *dst, const void *src, size_t n);
+void bc_par_memzero(void *dst, size_t n);
 void *bc_xrealloc(void *p, size_t n);
 void bc_mul_operands(const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p, bc_operand *oa, bc_operand *ob);
 /* Initialise the GPU engine once (aborts with a message if there is none). */

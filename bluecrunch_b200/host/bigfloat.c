@@ -149,16 +149,83 @@ static int64_t window(const _bigfloat_struct *a, const _bigfloat_struct *b, size
   return *top - (int64_t)p;
 }
 
+/* memcpy / memset of large arrays split over the OpenMP threads. */
+void bc_par_memcpy(void *dst, const void *src, size_t n) {
+  if (n < ((size_t)4 << 20)) {
+    memcpy(dst, src, n);
+    return;
+  }
+  const long nch = 64;
+  const size_t chunk = (n + (size_t)nch - 1) / (size_t)nch;
+#pragma omp parallel for schedule(static)
+  for (long h = 0; h < nch; h++) {
+    const size_t s0 = (size_t)h * chunk;
+    if (s0 < n) memcpy((char *)dst + s0, (const char *)src + s0, s0 + chunk < n ? chunk : n - s0);
+  }
+}
+
+void bc_par_memzero(void *dst, size_t n) {
+  if (n < ((size_t)4 << 20)) {
+    memset(dst, 0, n);
+    return;
+  }
+  const long nch = 64;
+  const size_t chunk = (n + (size_t)nch - 1) / (size_t)nch;
+#pragma omp parallel for schedule(static)
+  for (long h = 0; h < nch; h++) {
+    const size_t s0 = (size_t)h * chunk;
+    if (s0 < n) memset((char *)dst + s0, 0, s0 + chunk < n ? chunk : n - s0);
+  }
+}
+
+/* Sums and differences of more than PAR_LIMBS limbs run in parallel chunks:
+ * each chunk first with carry (borrow) in 0, recording its carry out and
+ * whether its result is all ones (all zeros), then the carries into the
+ * chunks follow in order (a chunk passes an incoming carry on only when its
+ * result is all ones), and each chunk that receives one adds it.  Same
+ * limbs as the serial loop. */
+#define PAR_LIMBS ((size_t)1 << 20)
+
 static void uadd(bigfloat_t t, const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p) {
   int64_t bot, top;
   int64_t e = window(a, b, p, &bot, &top);
   size_t n = (size_t)(top - bot);
   uint32_t *c = (uint32_t *)bc_xmalloc((n + 1) * sizeof(uint32_t));
   uint64_t carry = 0;
-  for (size_t i = 0; i < n; i++) {
-    uint64_t w = (uint64_t)limb_at(a, bot + (int64_t)i) + limb_at(b, bot + (int64_t)i) + carry;
-    c[i] = (uint32_t)w;
-    carry = w >> 32;
+  if (n < PAR_LIMBS) {
+    for (size_t i = 0; i < n; i++) {
+      uint64_t w = (uint64_t)limb_at(a, bot + (int64_t)i) + limb_at(b, bot + (int64_t)i) + carry;
+      c[i] = (uint32_t)w;
+      carry = w >> 32;
+    }
+  } else {
+    const long nch = 256;
+    const size_t chunk = (n + (size_t)nch - 1) / (size_t)nch;
+    unsigned char co[256], ones[256], ci[257];
+#pragma omp parallel for schedule(static)
+    for (long h = 0; h < nch; h++) {
+      const size_t s0 = (size_t)h * chunk, s1 = s0 + chunk < n ? s0 + chunk : n;
+      uint64_t cy = 0;
+      uint32_t all = 0xffffffffu;
+      for (size_t i = s0; i < s1; i++) {
+        uint64_t w = (uint64_t)limb_at(a, bot + (int64_t)i) + limb_at(b, bot + (int64_t)i) + cy;
+        c[i] = (uint32_t)w;
+        cy = w >> 32;
+        all &= c[i];
+      }
+      co[h] = (unsigned char)cy;
+      ones[h] = s0 < s1 && all == 0xffffffffu;
+    }
+    ci[0] = 0;
+    for (long h = 0; h < nch; h++) ci[h + 1] = co[h] | (ones[h] & ci[h]);
+#pragma omp parallel for schedule(static)
+    for (long h = 0; h < nch; h++) {
+      if (!ci[h]) continue;
+      const size_t s0 = (size_t)h * chunk, s1 = s0 + chunk < n ? s0 + chunk : n;
+      for (size_t i = s0; i < s1; i++)
+        if (++c[i] != 0) break;
+    }
+    carry = ci[nch];
   }
   if (carry) c[n++] = 1;
   int sign = a->sign;
@@ -175,11 +242,40 @@ static void usub(bigfloat_t t, const _bigfloat_struct *a, const _bigfloat_struct
   int64_t e = window(a, b, p, &bot, &top);
   size_t n = (size_t)(top - bot);
   uint32_t *c = (uint32_t *)bc_xmalloc((n + 1) * sizeof(uint32_t));
-  int64_t borrow = 0;
-  for (size_t i = 0; i < n; i++) {
-    int64_t w = (int64_t)limb_at(a, bot + (int64_t)i) - (int64_t)limb_at(b, bot + (int64_t)i) - borrow;
-    borrow = w < 0;
-    c[i] = (uint32_t)(w + (borrow ? ((int64_t)1 << 32) : 0));
+  if (n < PAR_LIMBS) {
+    int64_t borrow = 0;
+    for (size_t i = 0; i < n; i++) {
+      int64_t w = (int64_t)limb_at(a, bot + (int64_t)i) - (int64_t)limb_at(b, bot + (int64_t)i) - borrow;
+      borrow = w < 0;
+      c[i] = (uint32_t)(w + (borrow ? ((int64_t)1 << 32) : 0));
+    }
+  } else {
+    const long nch = 256;
+    const size_t chunk = (n + (size_t)nch - 1) / (size_t)nch;
+    unsigned char bo[256], zeros[256], bi[257];
+#pragma omp parallel for schedule(static)
+    for (long h = 0; h < nch; h++) {
+      const size_t s0 = (size_t)h * chunk, s1 = s0 + chunk < n ? s0 + chunk : n;
+      int64_t br = 0;
+      uint32_t any = 0;
+      for (size_t i = s0; i < s1; i++) {
+        int64_t w = (int64_t)limb_at(a, bot + (int64_t)i) - (int64_t)limb_at(b, bot + (int64_t)i) - br;
+        br = w < 0;
+        c[i] = (uint32_t)(w + (br ? ((int64_t)1 << 32) : 0));
+        any |= c[i];
+      }
+      bo[h] = (unsigned char)br;
+      zeros[h] = s0 < s1 && any == 0;
+    }
+    bi[0] = 0;
+    for (long h = 0; h < nch; h++) bi[h + 1] = bo[h] | (zeros[h] & bi[h]);
+#pragma omp parallel for schedule(static)
+    for (long h = 0; h < nch; h++) {
+      if (!bi[h]) continue;
+      const size_t s0 = (size_t)h * chunk, s1 = s0 + chunk < n ? s0 + chunk : n;
+      for (size_t i = s0; i < s1; i++)
+        if (c[i]-- != 0) break;
+    }
   }
   while (n > 0 && c[n - 1] == 0) n--;
   int sign = a->sign;

@@ -171,7 +171,7 @@ static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
     j = 0;
     size_t *slot = (size_t *)bc_xmalloc((m ? m : 1) * sizeof(size_t));
     for (size_t i = 0; i < m; i++) { slot[i] = j; j += L[i].c0 >= 0; }
-#pragma omp parallel for schedule(dynamic, 16)
+#pragma omp parallel for schedule(dynamic, 16) if (mm >= 64)  /* few big nodes: their adds run in parallel inside */
     for (long i = 0; i < mm; i++) {
       bnode *x = &L[i];
       if (x->c0 < 0) continue;

@@ -180,7 +180,7 @@ static void split_sizes(size_t k, size_t g, size_t *kh, size_t *kl, size_t *nh, 
 /* yh = top limbs of y (bigfloat/radix.c:245-249). */
 static void take_high(bigfloat_t yh, const _bigfloat_struct *y, size_t n, size_t nh) {
   bigfloat_alloc(yh, y->len - (n - nh));
-  memcpy(yh->coef, y->coef + (n - nh), yh->len * sizeof(uint32_t));
+  bc_par_memcpy(yh->coef, y->coef + (n - nh), yh->len * sizeof(uint32_t));
 }
 
 /* s = floor(sh/b) * b^kl + sl with the two edge fix-ups
@@ -196,8 +196,8 @@ static void merge(bigfloat_t s, bigfloat_t sh, const bigfloat_t sl, size_t kl) {
   }
   int sl_zero = sh->coef[0] == 0 && sl->coef[sl->len - 1] == NEWBASE - 1;
   bigfloat_alloc(s, sh->len - 1 + kl);
-  memset(s->coef, 0, kl * sizeof(uint32_t));
-  memcpy(s->coef + kl, sh->coef + 1, (sh->len - 1) * sizeof(uint32_t));
+  bc_par_memzero(s->coef, kl * sizeof(uint32_t));
+  bc_par_memcpy(s->coef + kl, sh->coef + 1, (sh->len - 1) * sizeof(uint32_t));
   if (!sl_zero) bigfloat_add(s, s, sl, 0);
 }
 
@@ -360,7 +360,7 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
   for (int d = nlv - 2; d >= 0; d--) {
     node *L = lv[d], *N = lv[d + 1];
     long m = (long)cnt[d];
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) if (m >= 16)  /* few big nodes: merge in parallel inside */
     for (long i = 0; i < m; i++) {
       node *x = &L[i];
       if (x->k <= KT) continue;

@@ -108,8 +108,9 @@ int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, b
 /* The binary-splitting sum of e's series on the GPU: P and Q with
  * P/Q = sum_{j=a+1}^{b} 1/((a+1)(a+2)...j) and Q = (a+1)(a+2)...b, the
  * integers the reference's e_BSR (main.c:63-109) builds on the host.  Every
- * intermediate value stays in device memory (leaves of 64 terms, then one
- * batched product level and one addition kernel per tree level).  On
+ * intermediate value stays in device memory (leaves of up to 1024 terms, one
+ * warp each, then one batched product level and one addition kernel per tree
+ * level).  On
  * success *P and *Q are malloc'd host arrays of *PL and *QL little-endian
  * limbs without top zeros (the caller frees them).  Needs b < 2^32 - 16. */
 int bc_gpu_e_series(uint32_t a, uint32_t b, uint32_t **P, size_t *PL, uint32_t **Q, size_t *QL);

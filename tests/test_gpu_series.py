@@ -39,7 +39,8 @@ def bc_err(r):
 
 
 @pytest.mark.parametrize("a,b", [(0, 1), (0, 2), (0, 63), (0, 64), (0, 65), (5, 77), (0, 1000), (1000, 1129),
-                                 (0, 20000), (123456, 160000), (0, 300000)])
+                                 (0, 1023), (0, 1024), (0, 1025), (0, 3073), (0, 20000), (123456, 160000),
+                                 (0, 300000), (2**31 - 5000, 2**31), (4000000000, 4000003000)])
 def test_series_exact(gpu, a, b):
     P, Q = _series(a, b)
     wp, wq = _exact(a, b)

@@ -116,3 +116,37 @@ def test_add_sub_truncation_semantics():
     assert t.len == 5 and t.exp == 1 - 5 and _val(t) == 7 << (32 * 4)
     lib.bigfloat_sub(t, x, y, 0)
     assert t.exp == -10 and t.len == 11 and t.sign == 1
+
+
+@pytest.mark.parametrize("kind", ["random", "carry_runs"])
+def test_long_add_sub_parallel_chunks(kind):
+    # bigfloat_add / bigfloat_sub above 2^20 limbs run in parallel chunks; the
+    # carry and borrow chains across chunk boundaries must match the serial loop
+    from bluecrunch_b200.bigfloat import Lib, value
+    import oracle
+    lib = Lib()
+    n = 1_500_000
+    a = oracle.random_limbs(77, n)
+    b = oracle.random_limbs(78, n - 5)
+    if kind == "carry_runs":
+        a[: n - 10] = 0xFFFFFFFF  # a carry from the bottom crosses every chunk
+        b[:] = 0
+        b[0] = 1
+    x, y = lib.make(a, exp=-3), lib.make(b, exp=-3)
+    t = lib.make()
+    lib.add(t, x, y, 0)
+    ia, ib = value(x)[2], value(y)[2]
+    s, e, v = value(t)
+    assert s == 1 and e == -3 and v == ia + ib
+    lib.sub(t, x, y, 0)
+    s, e, v = value(t)
+    assert s == 1 and e == -3 and v == ia - ib
+    # borrow through a long run of zeros
+    z = np.zeros(n, dtype=np.uint32)
+    z[-1] = 5
+    zz = lib.make(z, exp=-3)
+    one = lib.make(np.array([1], dtype=np.uint32), exp=-3)
+    lib.sub(t, zz, one, 0)
+    assert value(t)[2] == value(zz)[2] - 1
+    for q in (x, y, t, zz, one):
+        lib.free(q)
