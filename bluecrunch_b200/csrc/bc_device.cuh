@@ -106,6 +106,28 @@ __device__ __forceinline__ void dftR(double2 *x) {
 
 constexpr int PTS = 8;
 
+// Division of 32-bit values by a divisor fixed for a whole kernel, by one
+// multiply-high, a subtract, an add and two shifts (Granlund and
+// Montgomery, "Division by invariant integers using multiplication",
+// PLDI 1994, fig. 4.1): for 1 <= d < 2^32, l = ceil(log2 d),
+// m = floor(2^32 (2^l - d) / d) + 1, q = (t + ((n - t) >> min(l,1))) >> max(l-1,0)
+// with t = mulhi(m, n).  Built once per CTA; exact for every n < 2^32.
+struct FastDiv {
+  uint32_t d, m;
+  int s1, s2;
+  __host__ __device__ explicit FastDiv(uint32_t div) : d(div) {
+    int l = 0;
+    while (l < 32 && (1ull << l) < (unsigned long long)div) l++;
+    m = (uint32_t)((((1ull << l) - div) << 32) / div + 1);
+    s1 = l < 1 ? l : 1;
+    s2 = l - 1 > 0 ? l - 1 : 0;
+  }
+  __device__ __forceinline__ uint32_t div(uint32_t n) const {
+    const uint32_t t = __umulhi(m, n);
+    return (t + ((n - t) >> s1)) >> s2;
+  }
+};
+
 // Barrier policies for block_fft: the threads that exchange data through
 // shared memory in one transform.  CtaSync: the whole CTA.  GroupSync<N>:
 // the N threads (N a multiple of 32) of group g, on named barrier 1 + g;

@@ -362,9 +362,12 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
       const unsigned long long wend =
           min(it.nwords, (rt * (unsigned long long)nbits + (unsigned long long)nr * nbits + 31) / 32);
       const int nw = wend > w0 ? (int)(wend - w0) : 0;
+      // run of word i: 32i / (8b) = 4i / b = (4i * ceil(2^20/b)) >> 20, exact
+      // for 4i*b < 2^20 (here i < 6144 and b <= 24)
+      const unsigned rb = ((1u << 20) + (unsigned)it.b - 1) / (unsigned)it.b;
       for (int i = tid; i < nw; i += CARRY_NT) {
         const int bit = 32 * i;
-        const int k = bit / nbits, off = bit - k * nbits;
+        const int k = (int)((4u * (unsigned)i * rb) >> 20), off = bit - k * nbits;
         U192 hk = {{hc[k], hc[HC_STRIDE + k], hc[2 * HC_STRIDE + k]}};
         uint32_t x = u192_bits32(hk, off);
         if (off + 32 > nbits) {

@@ -120,12 +120,13 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
   const unsigned nops = (INV || p.sq) ? 1 : 2;
   const unsigned per_op = (unsigned)p.L1 * tiles, per_item = nops * per_op;
   const unsigned total = (unsigned)p.nitems * per_item;
+  const FastDiv fd_item(per_item), fd_op(per_op), fd_tile(tiles);
   auto decode = [&](unsigned u, int &item, int &op, int &blk, int &tile) {
-    item = (int)(u / per_item);
+    item = (int)fd_item.div(u);
     unsigned r = u - (unsigned)item * per_item;
-    op = (int)(r / per_op);
+    op = (int)fd_op.div(r);
     r -= (unsigned)op * per_op;
-    blk = (int)(r / tiles);
+    blk = (int)fd_tile.div(r);
     tile = (int)(r - (unsigned)blk * tiles);
   };
   auto issue = [&](unsigned u, int st) {
@@ -193,6 +194,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_i
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   const unsigned tiles = p.S1 / W;
   const unsigned total = (unsigned)p.nitems * tiles;  // far below 2^32
+  const FastDiv fd_tiles(tiles);
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -204,15 +206,17 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_i
   unsigned u = blockIdx.x;
   if (tid == 0 && u < total) {
     fence_proxy_async_smem();
-    tile_load_3d<L, W>(buf0, &mA, &bars[0], (int)(u % tiles) * W, (int)(u / tiles));
+    const unsigned q0 = fd_tiles.div(u);
+    tile_load_3d<L, W>(buf0, &mA, &bars[0], (int)(u - q0 * tiles) * W, (int)q0);
   }
   for (; u < total; u += gridDim.x) {
     const unsigned un = u + gridDim.x;
     if (tid == 0 && un < total) {
       fence_proxy_async_smem();
-      tile_load_3d<L, W>(buf0 + (st ^ 1) * L * W, &mA, &bars[st ^ 1], (int)(un % tiles) * W, (int)(un / tiles));
+      const unsigned qn = fd_tiles.div(un);
+      tile_load_3d<L, W>(buf0 + (st ^ 1) * L * W, &mA, &bars[st ^ 1], (int)(un - qn * tiles) * W, (int)qn);
     }
-    const int item = (int)(u / tiles), tile = (int)(u % tiles);
+    const int item = (int)fd_tiles.div(u), tile = (int)(u - (unsigned)item * tiles);
     const ItemDesc &it = p.items[item];
     const int col = tile * W + s;
     double2 v[PTS], w[PTS];
@@ -327,6 +331,7 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
   const int tid = threadIdx.x, rl = tid / TC, t = tid % TC;
   const unsigned rows_item = p.M / L;
   const unsigned total = (unsigned)p.nitems * rows_item / NR;  // far below 2^32
+  const FastDiv fd_rows(rows_item);
   if (tid == 0) {
 #pragma unroll
     for (int k = 0; k < 4; k++) mbar_init(&bars[k], 1);
@@ -351,7 +356,7 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
   for (int q = 0; u < total; u += gridDim.x, q = (q + 1 == NS) ? 0 : q + 1) {
     const unsigned un = u + NS * gridDim.x;  // the unit this slot loads next
     const unsigned grow = u * NR + rl;        // this thread's row in the class slab
-    const unsigned item = grow / rows_item;
+    const unsigned item = fd_rows.div(grow);
     const ItemDesc &it = p.items[item];
     double2 *ra = it.bufA + (grow - item * rows_item) * (unsigned)L;
     double2 *smA = bufA0 + q * NR * L + rl * L;
@@ -434,6 +439,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
   const int nops = p.sq ? 1 : 2;
   const unsigned per_item = (unsigned)(nops * tiles);
   const unsigned total = (unsigned)p.nitems * per_item;  // far below 2^32
+  const FastDiv fd_item(per_item), fd_tile((unsigned)tiles);
   // Row segment (n1, part) of tile tl starts one word below the word of digit
   // j0 = n1*S1 + tl*W + part*M.  S1 and M are multiples of 128, so that word is
   // n1*(S1 b/32) + part*(M b/32) + (tl*W*b >> 5), with the first two terms
@@ -444,8 +450,8 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     return al16 ? (int)((((long long)tl * W * b >> 5) - 1) & 3) : 0;
   };
   auto stage_copy = [&](unsigned u, int st) {
-    const int item = (int)(u / per_item), rem = (int)(u % per_item);
-    const int op = rem / tiles, tl = rem % tiles;
+    const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
+    const int op = (int)fd_tile.div((unsigned)rem), tl = rem - op * tiles;
     const ItemDesc &it = p.items[item];
     const uint32_t *X = op ? it.B : it.A;
     // word indices fit an int: operands and transforms stay below 2^29 words
@@ -455,8 +461,11 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     const int RW = (int)((unsigned)p.S1 * (unsigned)b / 32), PW = (int)((unsigned)p.M * (unsigned)b / 32);
     const int wbase = ((tl * W * b) >> 5) - 1 - seg_shift(tl, b, al16);
     uint32_t *dst = stg + st * K::STAGE_WORDS;
+    // the imaginary parts hold digits M and up: none when nd <= M
+    const int parts = (op ? it.ndB : it.ndA) > (unsigned long long)p.M ? 2 : 1;
     if (al16) {
-      constexpr int CH = K::SEGW4 / 4, NCH = 2 * L * CH;
+      constexpr int CH = K::SEGW4 / 4;
+      const int NCH = parts * L * CH;
       for (int idx = tid; idx < NCH; idx += NT) {
         const int segi = idx / CH, k = idx - segi * CH;
         const int part = segi >= L, row = segi - (part ? L : 0);
@@ -467,7 +476,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
         cp_async16(dst + segi * K::SEGW4 + 4 * k, X + (nv ? w : 0), nv * 4);
       }
     } else {
-      for (int idx = tid; idx < K::STAGE_WORDS; idx += NT) {
+      for (int idx = tid; idx < parts * (K::STAGE_WORDS / 2); idx += NT) {
         const int segi = idx / K::SEGW4, k = idx - segi * K::SEGW4;
         const int part = segi >= L, row = segi - (part ? L : 0);
         const int w = row * RW + (part ? PW : 0) + wbase + k;
@@ -486,8 +495,8 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    const int item = (int)(u / per_item), rem = (int)(u % per_item);
-    const int op = rem / tiles, tl = rem % tiles;
+    const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
+    const int op = (int)fd_tile.div((unsigned)rem), tl = rem - op * tiles;
     const ItemDesc &it = p.items[item];
     const unsigned nd = (unsigned)(op ? it.ndB : it.ndA);  // below 2^30
     double2 *gbuf = op ? it.bufB : it.bufA;
@@ -499,23 +508,33 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
                          (unsigned)(s * b);  // bit of digit j0+s in its staged segment
     const unsigned wi = (rel - 1) >> 5, sh = (rel - 1) & 31;
     const unsigned mask = (1u << b) - 1;
+    const bool imag = nd > (unsigned)p.M;  // any digit at M or above (else not staged)
+    // digit j of the operand from its staged segment (0 beyond nd)
+    auto digit = [&](int part, int n1) -> double {
+      const unsigned j = (unsigned)n1 * (unsigned)p.S1 + col + (part ? (unsigned)p.M : 0u);
+      const uint32_t *rw = seg + (part * L + n1) * K::SEGW4 + wi;
+      // bits [sh, sh+32) of the 64-bit window: the bit below the digit, then
+      // its b <= 24 bits
+      const unsigned x = __funnelshift_r(rw[0], rw[1], sh);
+      const int r = (int)((x >> 1) & mask);
+      const int top = (j + 1 >= nd) ? 0 : (r >> (b - 1));
+      return j < nd ? (double)(r - (top << b) + (int)(x & 1u)) : 0.0;
+    };
     double2 v[PTS];
+    if (imag) {
 #pragma unroll
-    for (int i = 0; i < PTS; i++) {
-      const int n1 = t + i * TC;
-      double d[2];
-#pragma unroll
-      for (int part = 0; part < 2; part++) {
-        const unsigned j = (unsigned)n1 * (unsigned)p.S1 + col + (part ? (unsigned)p.M : 0u);
-        const uint32_t *rw = seg + (part * L + n1) * K::SEGW4 + wi;
-        // bits [sh, sh+32) of the 64-bit window: the bit below the digit, then
-        // its b <= 24 bits
-        const unsigned x = __funnelshift_r(rw[0], rw[1], sh);
-        const int r = (int)((x >> 1) & mask);
-        const int top = (j + 1 >= nd) ? 0 : (r >> (b - 1));
-        d[part] = j < nd ? (double)(r - (top << b) + (int)(x & 1u)) : 0.0;
+      for (int i = 0; i < PTS; i++) {
+        const int n1 = t + i * TC;
+        v[i] = cmul(make_double2(digit(0, n1), digit(1, n1)), pwS[n1]);
       }
-      v[i] = cmul(make_double2(d[0], d[1]), pwS[n1]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < PTS; i++) {
+        const int n1 = t + i * TC;
+        const double d = digit(0, n1);
+        const double2 w = pwS[n1];
+        v[i] = make_double2(d * w.x, d * w.y);
+      }
     }
     block_fft<L, W, false>(v, t, s, tile, twS);
     double2 w[PTS];
