@@ -1202,6 +1202,26 @@ struct DevBuf {  // cudaMalloc'd, freed on scope exit
 };
 
 // ------------------------------------------------------------------ radix conversion leaves
+// Leaves whose fractions and digits are already in device memory, in one launch.
+int radix_leaves_device(const std::vector<RadixLeaf> &d, double alpha) {
+  if (d.empty()) return BC_OK;
+  const size_t o_flag = align256(d.size() * sizeof(RadixLeaf)), total = o_flag + 256;
+  int r = arena_reserve(total);
+  if (r) return r;
+  char *base = g.arena;
+  CK(cudaMemcpyAsync(base, d.data(), d.size() * sizeof(RadixLeaf), cudaMemcpyHostToDevice, g.stream));
+  CK(cudaMemsetAsync(base + o_flag, 0, 256, g.stream));
+  const unsigned grid =
+      (unsigned)std::min<size_t>((d.size() + RADIX_WARPS - 1) / RADIX_WARPS, (size_t)g.sm_count * 16);
+  k_radix_leaves<<<grid, 32 * RADIX_WARPS, 0, g.stream>>>((const RadixLeaf *)base, (int)d.size(), alpha,
+                                                          (unsigned *)(base + o_flag));
+  CK(cudaGetLastError());
+  unsigned flag = 0;
+  CK(cudaMemcpyAsync(&flag, base + o_flag, 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  return flag ? fail(BC_ERR_TOO_LARGE) : BC_OK;
+}
+
 // All leaves of one conversion in one launch: the fractions cross to the
 // device in one staged span, the digits come back in another.
 int radix_leaves_locked(const bc_radix_leaf *lv, size_t count, double alpha) {
@@ -1255,10 +1275,130 @@ int radix_leaves_locked(const bc_radix_leaf *lv, size_t count, double alpha) {
   return BC_OK;
 }
 
-int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vector<uint32_t> &hQ,
+// ------------------------------------------------------------------ radix conversion tree on the device
+// The conversion tree the caller planned (split sizes and power-table entry
+// per internal node, bigfloat/radix.c:228-318), run with every value in
+// device memory: top-down, one batch of products y * 10^(9(k-kl)) per depth;
+// the high child's fraction is a view of the top limbs of y, the low child's
+// a view of limbs [n - nl, n) of the product (zero-padded to n limbs, as the
+// reference's realloc pads it); all leaves in one launch; bottom-up, one
+// fix-up and one copy launch per depth for the merges.
+int radix_tree_locked(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nn,
+                      const uint32_t *const *table, const size_t *table_len, int ntable, double alpha,
+                      uint32_t *out) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (!y || !ylen || !nodes || !nn || !out || (ntable && (!table || !table_len))) return fail(BC_ERR_INVALID);
+  // depths (children come after their parent) and buffer sizes
+  std::vector<int> depth(nn, 0);
+  int maxd = 0;
+  std::vector<size_t> ylenv(nn, 0), prod_off(nn, SIZE_MAX), prod_len(nn, 0), s_off(nn);
+  ylenv[0] = ylen;
+  size_t prod_total = 0, s_total = 0;
+  for (size_t i = 0; i < nn; i++) {
+    const bc_radix_node &x = nodes[i];
+    s_off[i] = s_total;
+    s_total += (x.k + 63) & ~size_t(63);
+    if (x.child_h < 0) continue;
+    const size_t h = (size_t)x.child_h, l = (size_t)x.child_l;
+    if (h <= i || l <= i || h >= nn || l >= nn || x.table < 0 || x.table >= ntable) return fail(BC_ERR_INVALID);
+    depth[h] = depth[l] = depth[i] + 1;
+    maxd = std::max(maxd, depth[h]);
+    const size_t nh = nodes[h].n, nl = nodes[l].n;
+    if (nh > x.n || nl > x.n || ylenv[i] < x.n - nh) return fail(BC_ERR_INVALID);
+    ylenv[h] = ylenv[i] - (x.n - nh);
+    ylenv[l] = nl;
+    prod_len[i] = ylenv[i] + table_len[x.table];
+    prod_off[i] = prod_total;
+    prod_total += (std::max(prod_len[i], x.n) + 63) & ~size_t(63);
+  }
+  // device buffers: root fraction and table, products, digits
+  size_t tab_total = 0;
+  std::vector<size_t> tab_off(ntable);
+  for (int t = 0; t < ntable; t++) {
+    tab_off[t] = tab_total;
+    tab_total += (table_len[t] + 63) & ~size_t(63);
+  }
+  DevBuf din, dprod, ds, dmeta;
+  int r;
+  if ((r = din.alloc((((ylen + 63) & ~size_t(63)) + tab_total) * 4)) || (r = dprod.alloc(prod_total * 4)) ||
+      (r = ds.alloc(s_total * 4)))
+    return r;
+  uint32_t *dy = (uint32_t *)din.p, *dtab = dy + ((ylen + 63) & ~size_t(63));
+  {
+    std::vector<SpanJob> jobs;
+    jobs.push_back({0, (char *)y, ylen * 4});
+    for (int t = 0; t < ntable; t++)
+      if (table_len[t]) jobs.push_back({(((ylen + 63) & ~size_t(63)) + tab_off[t]) * 4, (char *)table[t], table_len[t] * 4});
+    if ((r = stage_h2d((char *)din.p, jobs, (((ylen + 63) & ~size_t(63)) + tab_total) * 4))) return r;
+  }
+  uint32_t *dp = (uint32_t *)dprod.p, *dsd = (uint32_t *)ds.p;
+  std::vector<const uint32_t *> yptr(nn, nullptr);
+  yptr[0] = dy;
+  // top-down products, one batch per depth
+  for (int d = 0; d < maxd; d++) {
+    std::vector<bc_mul_desc> md;
+    for (size_t i = 0; i < nn; i++) {
+      const bc_radix_node &x = nodes[i];
+      if (depth[i] != d || x.child_h < 0) continue;
+      uint32_t *C = dp + prod_off[i];
+      if (x.n > prod_len[i]) CK(cudaMemsetAsync(C + prod_len[i], 0, (x.n - prod_len[i]) * 4, g.stream));
+      md.push_back({C, prod_len[i], yptr[i], ylenv[i], dtab + tab_off[x.table], table_len[x.table]});
+      yptr[x.child_h] = yptr[i] + (x.n - nodes[x.child_h].n);
+      yptr[x.child_l] = C + (x.n - nodes[x.child_l].n);
+    }
+    bc_batch_stats st{};
+    if (!md.empty() && (r = mul_batch_locked(md.data(), md.size(), &st, nullptr, BC_BATCH_DEVICE_OPERANDS)))
+      return r;
+  }
+  // leaves
+  std::vector<RadixLeaf> lv;
+  for (size_t i = 0; i < nn; i++) {
+    const bc_radix_node &x = nodes[i];
+    if (x.child_h >= 0) continue;
+    if (ylenv[i] + 1 > (size_t)RADIX_WINDOW || x.n + 1 > (size_t)RADIX_WINDOW || x.n > ylenv[i] + 1 ||
+        x.k > 0xffffffffu)
+      return fail(BC_ERR_TOO_LARGE);
+    lv.push_back({yptr[i], dsd + s_off[i], (uint32_t)ylenv[i], (uint32_t)x.n, (uint32_t)x.k, 0u});
+  }
+  if ((r = radix_leaves_device(lv, alpha))) return r;
+  // bottom-up merges, one depth at a time
+  const size_t o_flag = align256(nn * sizeof(MergeDesc));
+  if ((r = dmeta.alloc(o_flag + nn * 4))) return r;
+  MergeDesc *dm = (MergeDesc *)dmeta.p;
+  unsigned *dflag = (unsigned *)((char *)dmeta.p + o_flag);
+  for (int d = maxd - 1; d >= 0; d--) {
+    std::vector<MergeDesc> mg;
+    unsigned long long units = 0;
+    for (size_t i = 0; i < nn; i++) {
+      const bc_radix_node &x = nodes[i];
+      if (depth[i] != d || x.child_h < 0) continue;
+      const size_t h = (size_t)x.child_h, l = (size_t)x.child_l;
+      const unsigned long long kh = nodes[h].k, kl = nodes[l].k;
+      if (kl != x.kl || kh + kl - 1 != x.k || kh == 0 || kl == 0) return fail(BC_ERR_INVALID);
+      mg.push_back({dsd + s_off[h], dsd + s_off[l], dsd + s_off[i], kh, kl, units});
+      units += (kh - 1 + kl + MERGE_UNIT - 1) / MERGE_UNIT;
+    }
+    if (mg.empty()) continue;
+    CK(cudaMemcpyAsync(dm, mg.data(), mg.size() * sizeof(MergeDesc), cudaMemcpyHostToDevice, g.stream));
+    k_merge_fix<<<(unsigned)((mg.size() + 127) / 128), 128, 0, g.stream>>>(dm, (int)mg.size(), dflag);
+    CK(cudaGetLastError());
+    const unsigned grid = (unsigned)std::min<unsigned long long>(units, (unsigned long long)g.sm_count * 8);
+    k_merge_copy<<<grid, 256, 0, g.stream>>>(dm, (int)mg.size(), units, dflag);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(g.stream));  // mg is rewritten for the next depth
+  }
+  // the root's digits
+  std::vector<SpanJob> jobs{{0, (char *)out, nodes[0].k * 4}};
+  if ((r = stage_d2h((const char *)(dsd + s_off[0]), jobs, nodes[0].k * 4))) return r;
+  CK(cudaStreamSynchronize(g.stream));
+  return BC_OK;
+}
+
+int e_series_locked(uint32_t a, uint32_t b, uint32_t **hP, size_t *PL, uint32_t **hQ, size_t *QL,
                     bc_batch_stats *st) {
   if (!g.init) return fail(BC_ERR_NOT_INIT);
   if (b <= a || b > 0xfffffff0u) return fail(BC_ERR_INVALID);
+  const auto t_start = std::chrono::steady_clock::now();
   // leaves as wide as a warp holds: T terms give at most T*bits(b)/32 + 1
   // limbs per value, which must stay within WLEAF_CAP
   int bits = 0;
@@ -1286,6 +1426,7 @@ int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vect
   auto secs = [](std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   };
+  const double t_leaves = secs(t_start);
   std::vector<DevNum> P(nleaf), Q(nleaf);
   for (uint32_t j = 0; j < nleaf; j++) {
     P[j] = {(uint32_t *)level.p + (size_t)(2 * j) * WLEAF_STRIDE, l0[2 * j]};
@@ -1395,12 +1536,29 @@ int e_series_locked(uint32_t a, uint32_t b, std::vector<uint32_t> &hP, std::vect
     Q.swap(Q2);
     std::swap(level.p, next.p);  // the old level is freed with `next`
   }
-  if (stats) fprintf(stderr, "      series: %u leaves, products %.3f s, lengths and sums %.3f s\n", nleaf, t_mul, t_add);
-  hP.resize(P[0].len);
-  hQ.resize(Q[0].len);
-  CK(cudaMemcpyAsync(hP.data(), P[0].p, P[0].len * 4, cudaMemcpyDeviceToHost, g.stream));
-  CK(cudaMemcpyAsync(hQ.data(), Q[0].p, Q[0].len * 4, cudaMemcpyDeviceToHost, g.stream));
-  CK(cudaStreamSynchronize(g.stream));
+  // the root's P and Q into malloc'd host arrays, through the pinned ring
+  const auto t_out = now();
+  *hP = (uint32_t *)malloc(std::max<size_t>(P[0].len, 1) * 4);
+  *hQ = (uint32_t *)malloc(std::max<size_t>(Q[0].len, 1) * 4);
+  if (!*hP || !*hQ) {
+    free(*hP);
+    free(*hQ);
+    *hP = *hQ = nullptr;
+    return fail(BC_ERR_NOMEM);
+  }
+  std::vector<SpanJob> jp{{0, (char *)*hP, P[0].len * 4}}, jq{{0, (char *)*hQ, Q[0].len * 4}};
+  if ((r = stage_d2h((const char *)P[0].p, jp, P[0].len * 4)) ||
+      (r = stage_d2h((const char *)Q[0].p, jq, Q[0].len * 4))) {
+    free(*hP);
+    free(*hQ);
+    *hP = *hQ = nullptr;
+    return r;
+  }
+  *PL = P[0].len;
+  *QL = Q[0].len;
+  if (stats)
+    fprintf(stderr, "      series: %u leaves %.3f s, products %.3f s, lengths and sums %.3f s, P and Q out %.3f s\n",
+            nleaf, t_leaves, t_mul, t_add, secs(t_out));
   return BC_OK;
 }
 
@@ -1499,23 +1657,16 @@ int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, b
 int bc_gpu_e_series(uint32_t a, uint32_t b, uint32_t **P, size_t *PL, uint32_t **Q, size_t *QL) {
   if (!P || !PL || !Q || !QL) return BC_ERR_INVALID;
   std::lock_guard<std::recursive_mutex> lk(g_mu);
-  std::vector<uint32_t> hp, hq;
   bc_batch_stats st{};
-  int r = e_series_locked(a, b, hp, hq, &st);
-  if (r) return r;
-  *P = (uint32_t *)malloc(std::max<size_t>(hp.size(), 1) * 4);
-  *Q = (uint32_t *)malloc(std::max<size_t>(hq.size(), 1) * 4);
-  if (!*P || !*Q) {
-    free(*P);
-    free(*Q);
-    *P = *Q = nullptr;
-    return fail(BC_ERR_NOMEM);
-  }
-  memcpy(*P, hp.data(), hp.size() * 4);
-  memcpy(*Q, hq.data(), hq.size() * 4);
-  *PL = hp.size();
-  *QL = hq.size();
-  return BC_OK;
+  *P = *Q = nullptr;
+  return e_series_locked(a, b, P, PL, Q, QL, &st);
+}
+
+int bc_gpu_radix_tree(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nnodes,
+                      const uint32_t *const *table, const size_t *table_len, int ntable, double alpha,
+                      uint32_t *out) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return radix_tree_locked(y, ylen, nodes, nnodes, table, table_len, ntable, alpha, out);
 }
 
 int bc_gpu_radix_leaves(const bc_radix_leaf *leaves, size_t count, double alpha) {

@@ -106,4 +106,55 @@ __global__ void __launch_bounds__(32 * RADIX_WARPS) k_radix_leaves(const RadixLe
   }
 }
 
+// ------------------------------------------------------------------ merges
+// An internal node's digits from its children's (the reference's merge,
+// bigfloat/radix.c:277-316): if the high part's lowest digit is 10^9 - 1 and
+// the low part's top digit is 0, add 1 to the high part (base 10^9, carry
+// past its top dropped); then the low kl digits are the low part's, or zero
+// when the high part's lowest digit is 0 and the low part's top digit is
+// 10^9 - 1; above them come the high part's digits from its second on.  No
+// other carry can arise: the sum in the reference adds the low part into
+// zeros.
+struct MergeDesc {
+  uint32_t *sh;        // kh digits of the high child (fixed in place)
+  const uint32_t *sl;  // kl digits of the low child
+  uint32_t *s;         // kh - 1 + kl digits of the node
+  unsigned long long kh, kl;
+  unsigned long long off;  // first copy unit of this node (batch-wide numbering)
+};
+
+// One thread per node: the +1 fix-up and the low-part decision (flag[i]).
+__global__ void k_merge_fix(MergeDesc *d, int n, unsigned *flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  MergeDesc m = d[i];
+  if (m.sh[0] == DEC_BASE - 1 && m.sl[m.kl - 1] == 0) {
+    unsigned long long carry = 1;
+    for (unsigned long long q = 0; q < m.kh && carry; q++) {
+      const unsigned long long v = (unsigned long long)m.sh[q] + carry;
+      carry = v / DEC_BASE;
+      m.sh[q] = (uint32_t)(v % DEC_BASE);
+    }
+  }
+  flag[i] = (m.sh[0] == 0 && m.sl[m.kl - 1] == DEC_BASE - 1) ? 1u : 0u;
+}
+
+// The copies, MERGE_UNIT digits per unit, units of all nodes in one grid.
+constexpr int MERGE_UNIT = 4096;
+__global__ void k_merge_copy(const MergeDesc *d, int n, unsigned long long units, const unsigned *flag) {
+  for (unsigned long long u = blockIdx.x; u < units; u += gridDim.x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (d[mid].off <= u) lo = mid; else hi = mid - 1;
+    }
+    const MergeDesc &m = d[lo];
+    const bool zero_low = flag[lo] != 0;
+    const unsigned long long len = m.kh - 1 + m.kl;
+    const unsigned long long i0 = (u - m.off) * MERGE_UNIT;
+    for (unsigned long long i = i0 + threadIdx.x; i < i0 + MERGE_UNIT && i < len; i += blockDim.x)
+      m.s[i] = i < m.kl ? (zero_low ? 0u : m.sl[i]) : m.sh[i - m.kl + 1];
+  }
+}
+
 }  // namespace bc

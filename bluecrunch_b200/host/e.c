@@ -82,10 +82,12 @@ static double wall_s(void) {
 
 /* mode 2: the series on the GPU, the root's P and Q back as bigfloats. */
 static void bsr_device(bigfloat_t P, bigfloat_t Q, uint32_t a, uint32_t b) {
+  double t0 = wall_s();
   bc_host_ensure_gpu();
+  if (getenv("BC_STATS")) printf("    GPU engine start: %.3f s\n", wall_s() - t0);
   uint32_t *p = NULL, *q = NULL;
   size_t pl = 0, ql = 0;
-  double t0 = wall_s();
+  t0 = wall_s();
   int rc = bc_gpu_e_series(a, b, &p, &pl, &q, &ql);
   if (rc != BC_OK) {
     fprintf(stderr, "bluecrunch: binary splitting on the GPU failed: %s\n", bc_gpu_strerror(rc));

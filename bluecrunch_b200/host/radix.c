@@ -9,12 +9,13 @@
  * fix-ups where the halves meet.  Every step that touches values is the same
  * as the reference's, so the digits are identical.
  *
- * Two drivers: convert_rec_percall() recurses like the reference (one GPU
- * product per node); convert_levels() walks the same tree level by level,
- * multiplies a whole level in one bigfloat_mul_batch, converts all leaves on
- * the GPU in one launch (bc_gpu_radix_leaves) and combines each level in
- * parallel on the host.  Both produce the same digits; bigfloat_radix uses
- * the level driver unless BC_RADIX_PERCALL is set.
+ * Three drivers, all producing the same digits: convert_rec_percall()
+ * recurses like the reference (one GPU product per node, BC_RADIX_PERCALL);
+ * convert_levels() walks the same tree level by level, multiplies a whole
+ * level in one bigfloat_mul_batch, converts all leaves on the GPU in one
+ * launch (bc_gpu_radix_leaves) and combines each level in parallel on the
+ * host (BC_RADIX_LEVELS); convert_tree(), the default, plans the tree here
+ * and runs all of it in device memory (bc_gpu_radix_tree).
  */
 #include <math.h>
 #include <stdio.h>
@@ -385,6 +386,55 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
   free(cnt);
 }
 
+/* ---------------------------------------------------------------- tree on the device */
+
+/* The same tree planned here (split_sizes, power-table entries) and run in
+ * one call, bc_gpu_radix_tree, with every product, leaf and merge in device
+ * memory: the fraction and the table go over once, the digits come back once. */
+static void convert_tree(bigfloat_t target, size_t k0, const _bigfloat_struct *y0, size_t n0, size_t g) {
+  double t0 = wall_now();
+  size_t cap = 64, nn = 1;
+  bc_radix_node *nd = (bc_radix_node *)bc_xmalloc(cap * sizeof(bc_radix_node));
+  nd[0].k = k0;
+  nd[0].n = n0;
+  nd[0].child_h = nd[0].child_l = -1;
+  nd[0].kl = 0;
+  nd[0].table = -1;
+  for (size_t i = 0; i < nn; i++) { /* breadth first: children after their parent */
+    if (nd[i].k <= KT) continue;
+    size_t kh, kl, nh, nl;
+    split_sizes(nd[i].k, g, &kh, &kl, &nh, &nl);
+    if (nn + 2 > cap) {
+      cap *= 2;
+      nd = (bc_radix_node *)bc_xrealloc(nd, cap * sizeof(bc_radix_node));
+    }
+    nd[i].kl = kl;
+    nd[i].table = table_find(&g_tab, nd[i].k - kl);
+    nd[i].child_h = (long)nn;
+    nd[i].child_l = (long)nn + 1;
+    bc_radix_node h = {kh, nh, -1, -1, 0, -1}, l = {kl, nl, -1, -1, 0, -1};
+    nd[nn++] = h;
+    nd[nn++] = l;
+  }
+  const uint32_t **tab = (const uint32_t **)bc_xmalloc((size_t)(g_tab.n ? g_tab.n : 1) * sizeof(uint32_t *));
+  size_t *tlen = (size_t *)bc_xmalloc((size_t)(g_tab.n ? g_tab.n : 1) * sizeof(size_t));
+  for (int t = 0; t < g_tab.n; t++) {
+    tab[t] = g_tab.val[t]->coef;
+    tlen[t] = g_tab.val[t]->len;
+  }
+  bigfloat_alloc(target, k0);
+  bc_host_ensure_gpu();
+  int rc = bc_gpu_radix_tree(y0->coef, y0->len, nd, nn, tab, tlen, g_tab.n, ALPHA, target->coef);
+  if (rc != BC_OK) {
+    fprintf(stderr, "bigfloat_radix: GPU conversion tree of %zu nodes failed: %s\n", nn, bc_gpu_strerror(rc));
+    abort();
+  }
+  if (getenv("BC_STATS")) printf("    conversion: %zu nodes on the device, %.3f s\n", nn, wall_now() - t0);
+  free(tab);
+  free(tlen);
+  free(nd);
+}
+
 /* bigfloat/radix.c:321-360 */
 void bigfloat_radix(bigfloat_t target, const bigfloat_t a) {
   if (-a->exp + 1 != (int64_t)a->len) {
@@ -401,7 +451,8 @@ void bigfloat_radix(bigfloat_t target, const bigfloat_t a) {
   bigfloat_alloc(target, k);
   task_start(2, "Conversion");
   if (getenv("BC_RADIX_PERCALL")) convert_rec_percall(target, k, a, n, g);
-  else convert_levels(target, k, a, n, g);
+  else if (getenv("BC_RADIX_LEVELS")) convert_levels(target, k, a, n, g);
+  else convert_tree(target, k, a, n, g);
   task_end(2);
   table_free(&g_tab);
   if (target->coef[target->len - 1] > NEWBASE) {

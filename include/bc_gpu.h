@@ -131,6 +131,24 @@ typedef struct {
 } bc_radix_leaf;
 int bc_gpu_radix_leaves(const bc_radix_leaf *leaves, size_t count, double alpha);
 
+/* The whole binary-to-decimal conversion tree of the reference's convert_rec
+ * (bigfloat/radix.c:228-318) on the GPU, as planned by the caller: node 0 is
+ * the root (k digits of the fraction y, n limbs below the point); an internal
+ * node names its high and low children (later in the array), the low
+ * child's digit count kl and the index of 10^(9(k-kl)) in `table`; a leaf
+ * has child_h = child_l = -1.  Every product, leaf and merge runs in device
+ * memory; y and the table entries cross once, the root's k digits come back
+ * into out (most significant last).  alpha as for bc_gpu_radix_leaves. */
+typedef struct {
+  size_t k, n;
+  long child_h, child_l;
+  size_t kl;
+  int table;
+} bc_radix_node;
+int bc_gpu_radix_tree(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nnodes,
+                      const uint32_t *const *table, const size_t *table_len, int ntable, double alpha,
+                      uint32_t *out);
+
 /* Launch on this CUDA stream (cudaStream_t as void*; NULL = library stream).
  * Calls still return only when their results are complete. */
 int bc_gpu_set_stream(void *stream);

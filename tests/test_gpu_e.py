@@ -34,6 +34,9 @@ def test_e_batched_matches_published_md5(digits):
     if digits <= 100000:
         md5, _, _ = _e(digits, levels=True)  # host tree, batched levels
         assert md5 == MD5[str(digits)]
+    if digits >= 100000:
+        md5, _, _ = _e(digits, env={"BC_RADIX_LEVELS": "1"})  # conversion levels merged on the host
+        assert md5 == MD5[str(digits)]
 
 
 def test_e_per_call_1e6_matches_batched():

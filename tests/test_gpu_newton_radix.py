@@ -29,14 +29,16 @@ def _lib():
 
 
 @pytest.mark.parametrize("case", GOLD, ids=lambda c: "n%d" % c["n"])
-@pytest.mark.parametrize("driver", ["levels", "percall"])
+@pytest.mark.parametrize("driver", ["tree", "levels", "percall"])
 def test_matches_reference(case, driver, monkeypatch):
+    monkeypatch.delenv("BC_RADIX_PERCALL", raising=False)
+    monkeypatch.delenv("BC_RADIX_LEVELS", raising=False)
     if driver == "percall":
         if case["n"] > 110_000:
             pytest.skip("per-call driver checked on the smaller cases")
         monkeypatch.setenv("BC_RADIX_PERCALL", "1")
-    else:
-        monkeypatch.delenv("BC_RADIX_PERCALL", raising=False)
+    elif driver == "levels":
+        monkeypatch.setenv("BC_RADIX_LEVELS", "1")
     lib = _lib()
     n = case["n"]
     xl, yl = operands(case["seed"], n)
@@ -97,6 +99,7 @@ def test_fifty_million_digits_verified():
     code = _BIG.format(root=ROOT, golden=os.path.join(ROOT, "tests", "golden"), n=n)
     env = dict(os.environ, BC_VERIFY="1")
     env.pop("BC_RADIX_PERCALL", None)
+    env.pop("BC_RADIX_LEVELS", None)
     p = subprocess.run([sys.executable, "-c", code], env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
                        text=True, timeout=900)
     assert p.returncode == 0, p.stderr[-2000:]
