@@ -27,6 +27,7 @@
 #include "bc_pipe.cuh"
 #include "bc_bsr.cuh"
 #include "bc_radix.cuh"
+#include "bc_rows_warp.cuh"
 
 using namespace bc;
 
@@ -120,6 +121,7 @@ struct Ctx {
   int last_error = 0;
   int last_cuda = 0;
   bool time_kernels = false;
+  bool rows_warp = true;  // 1024-point rows by k2_rows_w1024 ($BC_ROWS_WARP=0: the block kernel)
   std::vector<std::pair<const char *, double>> ktimes;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;
@@ -366,6 +368,7 @@ struct KInfo {
   int box = 0;            // TMA box lines (rows) the kernel expects per box
   unsigned unit_bytes = 0; // bytes the kernel waits for per staged unit (per operand)
   int parts = 1;          // boxes per column group (or per row)
+  bool warp_rows = false; // a row kernel with one warp per row and no tensor maps
 };
 
 template <int L>
@@ -418,6 +421,12 @@ KInfo get_mid(int L, bool inv) {
 #define ROWCASE(L) \
   case L: return sq ? rows_info<L, true>() : rows_info<L, false>();
 KInfo get_rows(int L, bool sq) {
+  if (L == RW_L && g.rows_warp) {
+    KInfo k{sq ? (const void *)k2_rows_w1024<true> : (const void *)k2_rows_w1024<false>, 32 * RW_WARPS, RW_SMEM,
+            "rows", SIG_P_MAP2};
+    k.warp_rows = true;
+    return k;
+  }
   switch (L) {
     ROWCASE(128) ROWCASE(192) ROWCASE(256) ROWCASE(384) ROWCASE(512) ROWCASE(768)
     ROWCASE(1024) ROWCASE(1536) ROWCASE(2048) ROWCASE(3072) ROWCASE(4096)
@@ -526,9 +535,9 @@ bool shape_launch_ok(const Shape &s, bool sq) {
   if (S1 % W1 || W1 % 8) return false;
   if ((size_t)(W1 / 8) * ki.parts * 128 * ki.box != ki.unit_bytes || (size_t)ki.box * ki.parts != (size_t)s.L1)
     return false;
-  const int NR = kr.threads / ((int)Lr / PTS);
-  if ((size_t)kr.parts * 128 * kr.box * NR != kr.unit_bytes || (size_t)kr.box * kr.parts != Lr / 8 ||
-      (s.M / Lr) % NR != 0 || kr.box > 256 || kr.box % 8)
+  const int NR = kr.warp_rows ? 1 : kr.threads / ((int)Lr / PTS);
+  if (!kr.warp_rows && ((size_t)kr.parts * 128 * kr.box * NR != kr.unit_bytes || (size_t)kr.box * kr.parts != Lr / 8 ||
+                        (s.M / Lr) % NR != 0 || kr.box > 256 || kr.box % 8))
     return false;
   if (s.levels == 3) {
     KInfo km = get_mid(s.L2, false);
@@ -570,7 +579,12 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
     if ((r = launch(km, n * nops * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB)))
       return r;
   }
-  {
+  if (get_rows(s.Lr, sq).warp_rows) {
+    // one warp per row, plain loads and stores: no tensor maps
+    KInfo kr = get_rows(s.Lr, sq);
+    const long long rows = n * (long long)(s.M / s.Lr);
+    if ((r = launch(kr, (rows + RW_WARPS - 1) / RW_WARPS, p, nl, stream, timed))) return r;
+  } else {
     KInfo kr = get_rows(s.Lr, sq);
     const int NR = kr.threads / (s.Lr / PTS);
     const cuuint64_t rows = (cuuint64_t)n * (cuuint64_t)(s.M / s.Lr);
@@ -1597,6 +1611,10 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
     atexit(print_profile);
   }
   g.verbose = c.verbose || getenv("BC_VERBOSE") != nullptr;
+  {
+    const char *rw = getenv("BC_ROWS_WARP");
+    g.rows_warp = !(rw && rw[0] == '0');
+  }
   load_width_file(c.tune_path);
   g.init = true;
   return BC_OK;
