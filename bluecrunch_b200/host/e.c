@@ -17,8 +17,13 @@
  * P and Q are the same integers in every mode (they do not depend on where
  * ranges split) and come out exponent 0 with no top zero limbs, as the
  * reference's products and additions leave them.
+ *
+ * The hex digits are formatted and written on a host thread while the
+ * radix conversion runs (it only reads e, as the conversion does); the
+ * "Writing hex digits" phase reports what is left of it afterwards.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -199,6 +204,24 @@ static void bsr_levels(bigfloat_t P, bigfloat_t Q, uint32_t a0, uint32_t b0) {
   free(cnt);
 }
 
+static int dump(const char *dir, const char *name, const char *s, size_t len);
+
+typedef struct {
+  const _bigfloat_struct *x;
+  size_t digits;
+  const char *outdir;
+  int rc;
+} hex_job;
+
+static void *hex_writer(void *arg) {
+  hex_job *j = (hex_job *)arg;
+  char *out = (char *)bc_xmalloc(j->digits + 22);
+  size_t len = bigfloat_to_string(out, j->x, j->digits, 16);
+  j->rc = dump(j->outdir, "e-hex.txt", out, len);
+  free(out);
+  return NULL;
+}
+
 static int dump(const char *dir, const char *name, const char *s, size_t len) {
   char path[4096];
   snprintf(path, sizeof path, "%s/%s", dir ? dir : ".", name);
@@ -249,12 +272,11 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   bigfloat_free(one);
   task_end(1);
 
-  task_start(1, "Writing hex digits");
   size_t out_len = digits + 2;
-  char *out = (char *)bc_xmalloc(out_len + 22);
-  size_t len = bigfloat_to_string(out, P, out_len, 16);
-  int rc = dump(outdir, "e-hex.txt", out, len);
-  task_end(1);
+  hex_job hj = {P, out_len, outdir, 0};
+  pthread_t hex_thread;
+  const int hex_async = pthread_create(&hex_thread, NULL, hex_writer, &hj) == 0;
+  if (!hex_async) hex_writer(&hj);
 
   task_start(1, "Converting to decimal");
   fflush(stdout);
@@ -263,8 +285,14 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   bigfloat_radix(dec, P);
   task_end(1);
 
+  task_start(1, "Writing hex digits");
+  if (hex_async) pthread_join(hex_thread, NULL);
+  int rc = hj.rc;
+  task_end(1);
+
   task_start(1, "Writing decimal digits");
-  len = bigfloat_to_string(out, dec, out_len, 10);
+  char *out = (char *)bc_xmalloc(out_len + 22);
+  size_t len = bigfloat_to_string(out, dec, out_len, 10);
   rc |= dump(outdir, "e.txt", out, len);
   bigfloat_free(P);
   bigfloat_free(dec);
