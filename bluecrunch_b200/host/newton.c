@@ -11,9 +11,17 @@
  */
 #include <stdio.h>
 #include <stdlib.h>
+#include <time.h>
 
 #include "bc_host.h"
 #include "bigfloat.h"
+
+/* $BC_STATS: per-level times of the large levels (products and subtractions). */
+static double now_s(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
 
 static void seed(bigfloat_t t, const bigfloat_t a) {
   int64_t e = a->exp;
@@ -62,10 +70,18 @@ void bigfloat_rcp(bigfloat_t t, const bigfloat_t a, size_t p) {
   bigfloat_new(corr);
   bigfloat_rcp(r, a, s);
   bigfloat_set(one, 1);
+  const int stats = p >= 1000000 && getenv("BC_STATS") != NULL;
+  double t0 = stats ? now_s() : 0, t1 = 0, t2 = 0, t3 = 0;
   bigfloat_mul(ax, a, r, p);       /* r*x */
+  if (stats) t1 = now_s();
   bigfloat_sub(err, ax, one, p);   /* r*x - 1 */
+  if (stats) t2 = now_s();
   bigfloat_mul(corr, err, r, p);   /* (r*x - 1)*r */
+  if (stats) t3 = now_s();
   bigfloat_sub(t, r, corr, p);     /* r - (r*x - 1)*r */
+  if (stats)
+    printf("    rcp level p=%zu: r*x %.3f s (%zu x %zu limbs), -1 %.3f s, *r %.3f s (%zu x %zu), r-corr %.3f s\n", p,
+           t1 - t0, a->len, r->len, t2 - t1, t3 - t2, err->len, r->len, now_s() - t3);
   bigfloat_free(r);
   bigfloat_free(one);
   bigfloat_free(ax);
@@ -78,6 +94,8 @@ void bigfloat_div(bigfloat_t t, const bigfloat_t a, const bigfloat_t b, size_t p
   bigfloat_new(r);
   if (p == 0) p = a->len + b->len;
   bigfloat_rcp(r, b, p);
+  const double t0 = now_s();
   bigfloat_mul(t, a, r, p);
+  if (p >= 1000000 && getenv("BC_STATS")) printf("    div: a*rcp %.3f s\n", now_s() - t0);
   bigfloat_free(r);
 }
