@@ -183,37 +183,138 @@ void bc_par_memzero(void *dst, size_t n) {
  * whether its result is all ones (all zeros), then the carries into the
  * chunks follow in order (a chunk passes an incoming carry on only when its
  * result is all ones), and each chunk that receives one adds it.  Same
- * limbs as the serial loop. */
+ * limbs as the serial loop.
+ *
+ * Inside a chunk the window is cut where an operand starts or ends, so each
+ * piece runs a plain loop over the operands present there (an absent
+ * operand contributes zeros) without a bounds test per limb. */
 #define PAR_LIMBS ((size_t)1 << 20)
+
+/* Output limb i of the window is limb i - off of x, for i in [lo, hi). */
+typedef struct {
+  const uint32_t *coef;
+  int64_t off;
+  size_t lo, hi;
+} opview;
+
+static opview view_of(const _bigfloat_struct *x, int64_t bot, size_t n) {
+  opview v;
+  const int64_t lo = x->exp - bot, hi = lo + (int64_t)x->len;
+  v.coef = x->coef;
+  v.off = lo;
+  v.lo = lo < 0 ? 0 : (lo > (int64_t)n ? n : (size_t)lo);
+  v.hi = hi < 0 ? 0 : (hi > (int64_t)n ? n : (size_t)hi);
+  if (v.hi < v.lo) v.hi = v.lo;
+  return v;
+}
+
+/* c[k] = A[k] + B[k] + cy over k < m (a null operand is zero); returns the
+ * carry out, ANDs the limbs into *all. */
+static uint64_t add_piece(uint32_t *c, const uint32_t *A, const uint32_t *B, size_t m, uint64_t cy, uint32_t *all) {
+  uint32_t al = *all;
+  if (A && B) {
+    for (size_t k = 0; k < m; k++) {
+      const uint64_t w = (uint64_t)A[k] + B[k] + cy;
+      c[k] = (uint32_t)w;
+      cy = w >> 32;
+      al &= c[k];
+    }
+  } else if (A || B) {
+    const uint32_t *X = A ? A : B;
+    for (size_t k = 0; k < m; k++) {
+      const uint64_t w = (uint64_t)X[k] + cy;
+      c[k] = (uint32_t)w;
+      cy = w >> 32;
+      al &= c[k];
+    }
+  } else {
+    for (size_t k = 0; k < m; k++) {
+      c[k] = (uint32_t)cy;
+      al &= c[k];
+      cy = 0;
+    }
+  }
+  *all = al;
+  return cy;
+}
+
+/* c[k] = A[k] - B[k] - br over k < m; returns the borrow out, ORs the limbs
+ * into *any. */
+static uint64_t sub_piece(uint32_t *c, const uint32_t *A, const uint32_t *B, size_t m, uint64_t br, uint32_t *any) {
+  uint32_t an = *any;
+  if (A && B) {
+    for (size_t k = 0; k < m; k++) {
+      const uint64_t w = (uint64_t)A[k] - B[k] - br;
+      c[k] = (uint32_t)w;
+      br = (w >> 32) & 1;
+      an |= c[k];
+    }
+  } else if (A) {
+    for (size_t k = 0; k < m; k++) {
+      const uint64_t w = (uint64_t)A[k] - br;
+      c[k] = (uint32_t)w;
+      br = (w >> 32) & 1;
+      an |= c[k];
+    }
+  } else if (B) {
+    for (size_t k = 0; k < m; k++) {
+      const uint64_t w = (uint64_t)0 - B[k] - br;
+      c[k] = (uint32_t)w;
+      br = (w >> 32) & 1;
+      an |= c[k];
+    }
+  } else {
+    for (size_t k = 0; k < m; k++) {
+      c[k] = br ? 0xffffffffu : 0u;
+      an |= c[k];
+    }
+  }
+  *any = an;
+  return br;
+}
+
+/* Limbs [s0, s1) of the window, cut at the operands' ends; `sub` selects
+ * a - b, else a + b.  Returns the carry (borrow) out; *acc collects the AND
+ * (sum) or OR (difference) of the limbs. */
+static uint64_t run_chunk(uint32_t *c, const opview *a, const opview *b, size_t s0, size_t s1, uint64_t cin, int sub,
+                          uint32_t *acc) {
+  size_t cut[6] = {s0, a->lo, a->hi, b->lo, b->hi, s1};
+  for (int i = 1; i < 6; i++)  /* insertion sort of six cut points */
+    for (int j = i; j > 0 && cut[j - 1] > cut[j]; j--) {
+      const size_t t = cut[j];
+      cut[j] = cut[j - 1];
+      cut[j - 1] = t;
+    }
+  uint64_t cy = cin;
+  for (int i = 0; i < 5; i++) {
+    size_t u = cut[i] < s0 ? s0 : cut[i], v = cut[i + 1] > s1 ? s1 : cut[i + 1];
+    if (u >= v) continue;
+    const uint32_t *A = (u >= a->lo && u < a->hi) ? a->coef + (int64_t)u - a->off : NULL;
+    const uint32_t *B = (u >= b->lo && u < b->hi) ? b->coef + (int64_t)u - b->off : NULL;
+    cy = sub ? sub_piece(c + u, A, B, v - u, cy, acc) : add_piece(c + u, A, B, v - u, cy, acc);
+  }
+  return cy;
+}
 
 static void uadd(bigfloat_t t, const _bigfloat_struct *a, const _bigfloat_struct *b, size_t p) {
   int64_t bot, top;
   int64_t e = window(a, b, p, &bot, &top);
   size_t n = (size_t)(top - bot);
   uint32_t *c = (uint32_t *)bc_xmalloc((n + 1) * sizeof(uint32_t));
+  const opview va = view_of(a, bot, n), vb = view_of(b, bot, n);
   uint64_t carry = 0;
   if (n < PAR_LIMBS) {
-    for (size_t i = 0; i < n; i++) {
-      uint64_t w = (uint64_t)limb_at(a, bot + (int64_t)i) + limb_at(b, bot + (int64_t)i) + carry;
-      c[i] = (uint32_t)w;
-      carry = w >> 32;
-    }
+    uint32_t all = 0xffffffffu;
+    carry = run_chunk(c, &va, &vb, 0, n, 0, 0, &all);
   } else {
     const long nch = 256;
     const size_t chunk = (n + (size_t)nch - 1) / (size_t)nch;
     unsigned char co[256], ones[256], ci[257];
 #pragma omp parallel for schedule(static)
     for (long h = 0; h < nch; h++) {
-      const size_t s0 = (size_t)h * chunk, s1 = s0 + chunk < n ? s0 + chunk : n;
-      uint64_t cy = 0;
+      const size_t s0 = (size_t)h * chunk < n ? (size_t)h * chunk : n, s1 = s0 + chunk < n ? s0 + chunk : n;
       uint32_t all = 0xffffffffu;
-      for (size_t i = s0; i < s1; i++) {
-        uint64_t w = (uint64_t)limb_at(a, bot + (int64_t)i) + limb_at(b, bot + (int64_t)i) + cy;
-        c[i] = (uint32_t)w;
-        cy = w >> 32;
-        all &= c[i];
-      }
-      co[h] = (unsigned char)cy;
+      co[h] = (unsigned char)run_chunk(c, &va, &vb, s0, s1, 0, 0, &all);
       ones[h] = s0 < s1 && all == 0xffffffffu;
     }
     ci[0] = 0;
@@ -242,29 +343,19 @@ static void usub(bigfloat_t t, const _bigfloat_struct *a, const _bigfloat_struct
   int64_t e = window(a, b, p, &bot, &top);
   size_t n = (size_t)(top - bot);
   uint32_t *c = (uint32_t *)bc_xmalloc((n + 1) * sizeof(uint32_t));
+  const opview va = view_of(a, bot, n), vb = view_of(b, bot, n);
   if (n < PAR_LIMBS) {
-    int64_t borrow = 0;
-    for (size_t i = 0; i < n; i++) {
-      int64_t w = (int64_t)limb_at(a, bot + (int64_t)i) - (int64_t)limb_at(b, bot + (int64_t)i) - borrow;
-      borrow = w < 0;
-      c[i] = (uint32_t)(w + (borrow ? ((int64_t)1 << 32) : 0));
-    }
+    uint32_t any = 0;
+    (void)run_chunk(c, &va, &vb, 0, n, 0, 1, &any);
   } else {
     const long nch = 256;
     const size_t chunk = (n + (size_t)nch - 1) / (size_t)nch;
     unsigned char bo[256], zeros[256], bi[257];
 #pragma omp parallel for schedule(static)
     for (long h = 0; h < nch; h++) {
-      const size_t s0 = (size_t)h * chunk, s1 = s0 + chunk < n ? s0 + chunk : n;
-      int64_t br = 0;
+      const size_t s0 = (size_t)h * chunk < n ? (size_t)h * chunk : n, s1 = s0 + chunk < n ? s0 + chunk : n;
       uint32_t any = 0;
-      for (size_t i = s0; i < s1; i++) {
-        int64_t w = (int64_t)limb_at(a, bot + (int64_t)i) - (int64_t)limb_at(b, bot + (int64_t)i) - br;
-        br = w < 0;
-        c[i] = (uint32_t)(w + (br ? ((int64_t)1 << 32) : 0));
-        any |= c[i];
-      }
-      bo[h] = (unsigned char)br;
+      bo[h] = (unsigned char)run_chunk(c, &va, &vb, s0, s1, 0, 1, &any);
       zeros[h] = s0 < s1 && any == 0;
     }
     bi[0] = 0;

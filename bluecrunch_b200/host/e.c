@@ -22,12 +22,14 @@
  * radix conversion runs (it only reads e, as the conversion does); the
  * "Writing hex digits" phase reports what is left of it afterwards.
  */
+#include <fcntl.h>
 #include <math.h>
 #include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
+#include <unistd.h>
 
 #include "bc_gpu.h"
 #include "bc_host.h"
@@ -222,9 +224,40 @@ static void *hex_writer(void *arg) {
   return NULL;
 }
 
+/* Outputs of 64 MiB and more are written by several threads, each with
+ * pwrite at its own offset (the copy into the page cache is most of the
+ * time of a gigabyte-sized write). */
 static int dump(const char *dir, const char *name, const char *s, size_t len) {
   char path[4096];
   snprintf(path, sizeof path, "%s/%s", dir ? dir : ".", name);
+  if (len >= ((size_t)64 << 20)) {
+    const int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0) {
+      fprintf(stderr, "Cannot create file %s\n", path);
+      return -1;
+    }
+    const long nch = 16;
+    const size_t chunk = (len + (size_t)nch - 1) / (size_t)nch;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long h = 0; h < nch; h++) {
+      size_t off = (size_t)h * chunk;
+      const size_t end = off + chunk < len ? off + chunk : len;
+      while (off < end) {
+        const ssize_t w = pwrite(fd, s + off, end - off, (off_t)off);
+        if (w <= 0) {
+          bad = 1;
+          break;
+        }
+        off += (size_t)w;
+      }
+    }
+    if (close(fd) != 0 || bad) {
+      fprintf(stderr, "Cannot write file %s\n", path);
+      return -1;
+    }
+    return 0;
+  }
   FILE *f = fopen(path, "wb");
   if (!f) {
     fprintf(stderr, "Cannot create file %s\n", path);

@@ -150,3 +150,61 @@ def test_long_add_sub_parallel_chunks(kind):
     assert value(t)[2] == value(zz)[2] - 1
     for q in (x, y, t, zz, one):
         lib.free(q)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_add_sub_windows_random(seed):
+    # random operand placements (overlapping, nested, disjoint with a gap),
+    # lengths on both sides of the 2^20-limb parallel threshold and
+    # precisions that cut into either operand, against Python integers: the
+    # limbs are the exact sum / difference of the operands' limbs at or
+    # above bot = top - (p + 2) (all limbs when p = 0)
+    # (bigfloat/addsub.c:65-181)
+    from bluecrunch_b200.bigfloat import Lib, value
+    import oracle
+    lib = Lib()
+    rng = np.random.default_rng(1000 + seed)
+    big = seed >= 4
+    for case in range(4 if big else 40):
+        la = int(rng.integers(1, 3_000_000 if big else 300))
+        lb = int(rng.integers(1, 3_000_000 if big else 300))
+        ea = int(rng.integers(-2 * la, la))
+        eb = ea + int(rng.integers(-la - lb - 50, la + lb + 50))
+        a = oracle.random_limbs(seed * 1000 + 2 * case, la)
+        b = oracle.random_limbs(seed * 1000 + 2 * case + 1, lb)
+        a[-1] |= 1
+        b[-1] |= 1
+        if case % 3 == 0:
+            a[: la // 2] = 0xFFFFFFFF  # long carry and borrow runs
+        x, y, t = lib.make(a, exp=ea), lib.make(b, exp=eb), lib.make()
+        top = max(ea + la, eb + lb)
+        bot_full = min(ea, eb)
+        p = 0 if case % 2 == 0 else int(rng.integers(1, top - bot_full + 3))
+        bot = bot_full if p == 0 or top - bot_full <= p + 2 else top - (p + 2)
+        # the result's exponent is top - (p + 2) whenever p > 0, also when
+        # nothing was cut (the reference sets it so, bigfloat/addsub.c:108,
+        # and its limbs still start at bot)
+        e_want = bot_full if p == 0 else top - (p + 2)
+
+        def trunc(limbs, e):
+            k = max(0, bot - e)
+            if k >= len(limbs):
+                return 0
+            return int.from_bytes(limbs[k:].astype("<u4").tobytes(), "little") << (32 * (e + k - bot))
+
+        ia, ib = trunc(a, ea), trunc(b, eb)
+        lib.add(t, x, y, p)
+        s, e, v = value(t)
+        assert (s, e, v) == (1, e_want, ia + ib), (case, la, lb, ea, eb, p)
+        lib.sub(t, x, y, p)
+        s, e, v = value(t)
+        full_a = int.from_bytes(a.astype("<u4").tobytes(), "little") << (32 * (ea - bot_full))
+        full_b = int.from_bytes(b.astype("<u4").tobytes(), "little") << (32 * (eb - bot_full))
+        if full_a == full_b:
+            continue
+        want = ia - ib if full_a > full_b else ib - ia
+        if want:
+            # sign field: 1 positive, 0 negative (include/bigfloat.h)
+            assert (e, v) == (e_want, want) and s == (1 if full_a > full_b else 0), (case, la, lb, ea, eb, p)
+        for q in (x, y, t):
+            lib.free(q)
