@@ -41,6 +41,46 @@ def test_three_level(gpu, orc, al):
     _check(gpu, orc, limbs(al + 17, al), limbs(al + 19, al))
 
 
+@pytest.mark.parametrize("al,bl,sq", [(1 << 21, 1 << 21, False), (1 << 22, 1 << 22, False), (1 << 22, 1 << 19, False),
+                                      (1 << 22, 1 << 22, True), (3 << 20, 3 << 20, False)])
+def test_three_level_rows_of_1024(gpu, orc, al, bl, sq):
+    # transforms of 2^22 and more points run their 1024-point rows on the
+    # one-warp-per-row kernel (k2_rows_w1024), squaring included
+    a = limbs(al + 29, al)
+    b = a if sq else limbs(bl + 31, bl)
+    st = _check(gpu, orc, a, b, square=sq)
+    assert st["fft_points"] >= 1 << 21
+
+
+_ROWS_BLOCK = r"""
+import sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {tests!r})
+import numpy as np
+import bluecrunch_b200 as bc
+import oracle
+from conftest import limbs
+bc.init(0)
+n = 1 << 21
+a, b = limbs(101, n), limbs(102, n)
+c = bc.mul(a, b, CL=2 * n)
+assert np.array_equal(c, oracle.restated().ntt_mul(a, b, 2 * n))
+s = bc.mul(a, None, CL=2 * n, square=True)
+assert np.array_equal(s, oracle.restated().ntt_mul(a, a, 2 * n))
+print("OK")
+"""
+
+
+def test_block_row_kernel_for_1024_point_rows():
+    # BC_ROWS_WARP=0 keeps the 8-points-per-thread row kernel k2_rows<1024>
+    import subprocess
+    import sys
+    root = os.path.dirname(HERE)
+    env = dict(os.environ, BC_ROWS_WARP="0")
+    p = subprocess.run([sys.executable, "-c", _ROWS_BLOCK.format(root=root, tests=HERE)], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0 and p.stdout.strip().endswith("OK"), p.stderr[-2000:]
+
+
 @pytest.mark.parametrize("n", [100, 2048, 30000, 1 << 18, 1 << 20])
 def test_squaring(gpu, orc, n):
     a = limbs(n + 23, n)
