@@ -125,6 +125,11 @@ struct Ctx {
   std::vector<std::pair<const char *, double>> ktimes;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;
+  std::vector<cudaEvent_t> kev_pool;  // recycled timing events
+  // pinned host blocks for the per-call descriptor upload and verdict
+  // readback (copies from pinned memory need no staging by the driver)
+  void *pin_small = nullptr;
+  size_t pin_small_cap = 0;
   int sm_count = 148;
 };
 
@@ -474,7 +479,12 @@ int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunc
   (*nlaunch)++;
   if (timed && g.time_kernels) {
     cudaEvent_t e;
-    CK(cudaEventCreate(&e));
+    if (!g.kev_pool.empty()) {
+      e = g.kev_pool.back();
+      g.kev_pool.pop_back();
+    } else {
+      CK(cudaEventCreate(&e));
+    }
     CK(cudaEventRecord(e, stream));
     g.kev.push_back(e);
     g.ktimes.push_back({k.name, 0.0});
@@ -874,6 +884,22 @@ int stage_d2h(const char *dev, const std::vector<SpanJob> &jobs, size_t total) {
 
 // Run one attempt over `works` (none done yet).  Fills err/flags and copies
 // out the products that pass the rounding check.
+// A pinned host block of at least `bytes` (grown on demand; its previous
+// contents are not kept).
+int pin_small_reserve(size_t bytes) {
+  if (bytes <= g.pin_small_cap) return BC_OK;
+  if (g.pin_small) {
+    CK(cudaStreamSynchronize(g.stream));
+    CK(cudaFreeHost(g.pin_small));
+    g.pin_small = nullptr;
+    g.pin_small_cap = 0;
+  }
+  const size_t want = std::max<size_t>(align256(bytes), 64 << 10);
+  CK(cudaHostAlloc(&g.pin_small, want, cudaHostAllocDefault));
+  g.pin_small_cap = want;
+  return BC_OK;
+}
+
 int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st, unsigned flags_in) {
   const bool all_host = flags_in & BC_BATCH_HOST_OPERANDS;
   const bool all_dev = flags_in & BC_BATCH_DEVICE_OPERANDS;
@@ -1022,7 +1048,12 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     }
   }
   ItemDesc *ddesc = (ItemDesc *)(base + off_desc);
-  CK(cudaMemcpyAsync(ddesc, desc.data(), nw * sizeof(ItemDesc), cudaMemcpyHostToDevice, g.stream));
+  // descriptors and, later, the verdicts go through one pinned block: the
+  // descriptors at its start, the verdicts (err, flags) after them
+  const size_t pin_desc = align256(nw * sizeof(ItemDesc)), pin_verd = off_flags + nw * 4 - off_err;
+  if ((r = pin_small_reserve(pin_desc + pin_verd))) return r;
+  memcpy(g.pin_small, desc.data(), nw * sizeof(ItemDesc));
+  CK(cudaMemcpyAsync(ddesc, g.pin_small, nw * sizeof(ItemDesc), cudaMemcpyHostToDevice, g.stream));
   unsigned int *ctr = (unsigned int *)(base + off_ctr);
 
   // ---- launches
@@ -1056,12 +1087,14 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   st->classes += classes.size();
 
   // ---- verdicts, then outputs of the products that passed
-  std::vector<unsigned long long> errs(nw);
-  std::vector<unsigned> flags(nw);
-  CK(cudaMemcpyAsync(errs.data(), base + off_err, nw * 8, cudaMemcpyDeviceToHost, g.stream));
-  CK(cudaMemcpyAsync(flags.data(), base + off_flags, nw * 4, cudaMemcpyDeviceToHost, g.stream));
+  char *verd = (char *)g.pin_small + pin_desc;
+  CK(cudaMemcpyAsync(verd, base + off_err, pin_verd, cudaMemcpyDeviceToHost, g.stream));
   pt.next(&g_prof.wait);
   CK(cudaStreamSynchronize(g.stream));
+  std::vector<unsigned long long> errs(nw);
+  std::vector<unsigned> flags(nw);
+  memcpy(errs.data(), verd, nw * 8);
+  memcpy(flags.data(), verd + (off_flags - off_err), nw * 4);
   pt.next(&g_prof.copy_out);
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, g.ev0, g.ev1));
@@ -1074,7 +1107,7 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
       g.ktimes[g.ktimes.size() - g.kev.size() + k].second = km;
       prev = g.kev[k];
     }
-    for (auto e : g.kev) cudaEventDestroy(e);
+    for (auto e : g.kev) g.kev_pool.push_back(e);
     g.kev.clear();
   }
   bool copies = false, staged_out = false;
@@ -1629,6 +1662,11 @@ int bc_gpu_shutdown(void) {
   if (g.arena) cudaFree(g.arena);
   g.arena = nullptr;
   g.arena_cap = 0;
+  for (auto e : g.kev_pool) cudaEventDestroy(e);
+  g.kev_pool.clear();
+  if (g.pin_small) cudaFreeHost(g.pin_small);
+  g.pin_small = nullptr;
+  g.pin_small_cap = 0;
   if (g.ev0) cudaEventDestroy(g.ev0);
   if (g.ev1) cudaEventDestroy(g.ev1);
   if (g.own_stream) cudaStreamDestroy(g.own_stream);
