@@ -327,15 +327,9 @@ def gpu_arm(args):
     import bluecrunch_b200 as bc
     import oracle
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from bluecrunch_b200.replicas import Replicas, job_throughput
+    reps = Replicas()  # N ranks = N independent replicas; no collective on the data path
+    world, rank, local = reps.world, reps.rank, reps.local
     torch.cuda.set_device(local)
     bc.init(local)
     stream = torch.cuda.current_stream()
@@ -360,8 +354,7 @@ def gpu_arm(args):
     assert oracle.restated().modcheck(host_c, a, b, 4), "GPU product fails the modular check"
 
     def barrier():
-        if dist:
-            dist.barrier()
+        reps.barrier()
         torch.cuda.synchronize()
 
     for _ in range(W):
@@ -391,11 +384,8 @@ def gpu_arm(args):
     bc.time_kernels(False)
     barrier()
     launches = K * per_product  # kernels of this library launched in the timed pass
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = nbytes * world / (ms * 1e-3) / 1e9
+    ms = reps.max(ms)
+    value = job_throughput(nbytes, ms, world) / 1e9
 
     # ---- e2e: pinned host buffers through the C ABI, copies in the timed region
     ha = torch.from_numpy(a.view(np.int32)).pin_memory()
@@ -406,13 +396,9 @@ def gpu_arm(args):
     t0 = time.perf_counter()
     for _ in range(max(1, K)):
         bc.mul(ha, hb, CL=CL, out=hc)
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / max(1, K)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = reps.max((time.perf_counter() - t0) * 1e3 / max(1, K))
     assert np.array_equal(hc.numpy().view(np.uint32), host_c)
-    e2e = nbytes * world / (e2e_ms * 1e-3) / 1e9
+    e2e = job_throughput(nbytes, e2e_ms, world) / 1e9
 
     # ---- roofline of the dominant kernel (algorithmic bytes per launch)
     M = p["fft_points"]
@@ -540,9 +526,7 @@ def gpu_arm(args):
             "e": e_runs,
         }
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
 
 
 def main():
