@@ -126,7 +126,7 @@ struct Ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;
   std::vector<cudaEvent_t> kev_pool;  // recycled timing events
-  // pinned host blocks for the per-call descriptor upload and verdict
+  // pinned host blocks for the per-call descriptor upload and outcome
   // readback (copies from pinned memory need no staging by the driver)
   void *pin_small = nullptr;
   size_t pin_small_cap = 0;
@@ -1048,10 +1048,10 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     }
   }
   ItemDesc *ddesc = (ItemDesc *)(base + off_desc);
-  // descriptors and, later, the verdicts go through one pinned block: the
-  // descriptors at its start, the verdicts (err, flags) after them
-  const size_t pin_desc = align256(nw * sizeof(ItemDesc)), pin_verd = off_flags + nw * 4 - off_err;
-  if ((r = pin_small_reserve(pin_desc + pin_verd))) return r;
+  // descriptors and, later, the outcomes go through one pinned block: the
+  // descriptors at its start, the outcomes (err, flags) after them
+  const size_t pin_desc = align256(nw * sizeof(ItemDesc)), pin_outc = off_flags + nw * 4 - off_err;
+  if ((r = pin_small_reserve(pin_desc + pin_outc))) return r;
   memcpy(g.pin_small, desc.data(), nw * sizeof(ItemDesc));
   CK(cudaMemcpyAsync(ddesc, g.pin_small, nw * sizeof(ItemDesc), cudaMemcpyHostToDevice, g.stream));
   unsigned int *ctr = (unsigned int *)(base + off_ctr);
@@ -1086,15 +1086,15 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   CK(cudaEventRecord(g.ev1, g.stream));
   st->classes += classes.size();
 
-  // ---- verdicts, then outputs of the products that passed
-  char *verd = (char *)g.pin_small + pin_desc;
-  CK(cudaMemcpyAsync(verd, base + off_err, pin_verd, cudaMemcpyDeviceToHost, g.stream));
+  // ---- outcomes, then outputs of the products that passed
+  char *outc = (char *)g.pin_small + pin_desc;
+  CK(cudaMemcpyAsync(outc, base + off_err, pin_outc, cudaMemcpyDeviceToHost, g.stream));
   pt.next(&g_prof.wait);
   CK(cudaStreamSynchronize(g.stream));
   std::vector<unsigned long long> errs(nw);
   std::vector<unsigned> flags(nw);
-  memcpy(errs.data(), verd, nw * 8);
-  memcpy(flags.data(), verd + (off_flags - off_err), nw * 4);
+  memcpy(errs.data(), outc, nw * 8);
+  memcpy(flags.data(), outc + (off_flags - off_err), nw * 4);
   pt.next(&g_prof.copy_out);
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, g.ev0, g.ev1));
