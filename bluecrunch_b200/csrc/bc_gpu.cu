@@ -1330,11 +1330,12 @@ int radix_leaves_locked(const bc_radix_leaf *lv, size_t count, double alpha) {
 // a view of limbs [n - nl, n) of the product (zero-padded to n limbs, as the
 // reference's realloc pads it); all leaves in one launch; bottom-up, one
 // fix-up and one copy launch per depth for the merges.
-int radix_tree_locked(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nn,
-                      const uint32_t *const *table, const size_t *table_len, int ntable, double alpha,
-                      uint32_t *out) {
+// The tree on device operands: dy (ylen limbs) and the table entries
+// dtab[t] (table_len[t] limbs) are in device memory.
+int radix_tree_core(const uint32_t *dy, size_t ylen, const bc_radix_node *nodes, size_t nn,
+                    const uint32_t *const *dtab, const size_t *table_len, int ntable, double alpha, uint32_t *out) {
   if (!g.init) return fail(BC_ERR_NOT_INIT);
-  if (!y || !ylen || !nodes || !nn || !out || (ntable && (!table || !table_len))) return fail(BC_ERR_INVALID);
+  if (!dy || !ylen || !nodes || !nn || !out || (ntable && (!dtab || !table_len))) return fail(BC_ERR_INVALID);
   // depths (children come after their parent) and buffer sizes
   std::vector<int> depth(nn, 0);
   int maxd = 0;
@@ -1358,26 +1359,10 @@ int radix_tree_locked(const uint32_t *y, size_t ylen, const bc_radix_node *nodes
     prod_off[i] = prod_total;
     prod_total += (std::max(prod_len[i], x.n) + 63) & ~size_t(63);
   }
-  // device buffers: root fraction and table, products, digits
-  size_t tab_total = 0;
-  std::vector<size_t> tab_off(ntable);
-  for (int t = 0; t < ntable; t++) {
-    tab_off[t] = tab_total;
-    tab_total += (table_len[t] + 63) & ~size_t(63);
-  }
-  DevBuf din, dprod, ds, dmeta;
+  // device buffers: products, digits
+  DevBuf dprod, ds, dmeta;
   int r;
-  if ((r = din.alloc((((ylen + 63) & ~size_t(63)) + tab_total) * 4)) || (r = dprod.alloc(prod_total * 4)) ||
-      (r = ds.alloc(s_total * 4)))
-    return r;
-  uint32_t *dy = (uint32_t *)din.p, *dtab = dy + ((ylen + 63) & ~size_t(63));
-  {
-    std::vector<SpanJob> jobs;
-    jobs.push_back({0, (char *)y, ylen * 4});
-    for (int t = 0; t < ntable; t++)
-      if (table_len[t]) jobs.push_back({(((ylen + 63) & ~size_t(63)) + tab_off[t]) * 4, (char *)table[t], table_len[t] * 4});
-    if ((r = stage_h2d((char *)din.p, jobs, (((ylen + 63) & ~size_t(63)) + tab_total) * 4))) return r;
-  }
+  if ((r = dprod.alloc(prod_total * 4)) || (r = ds.alloc(s_total * 4))) return r;
   uint32_t *dp = (uint32_t *)dprod.p, *dsd = (uint32_t *)ds.p;
   std::vector<const uint32_t *> yptr(nn, nullptr);
   yptr[0] = dy;
@@ -1389,7 +1374,7 @@ int radix_tree_locked(const uint32_t *y, size_t ylen, const bc_radix_node *nodes
       if (depth[i] != d || x.child_h < 0) continue;
       uint32_t *C = dp + prod_off[i];
       if (x.n > prod_len[i]) CK(cudaMemsetAsync(C + prod_len[i], 0, (x.n - prod_len[i]) * 4, g.stream));
-      md.push_back({C, prod_len[i], yptr[i], ylenv[i], dtab + tab_off[x.table], table_len[x.table]});
+      md.push_back({C, prod_len[i], yptr[i], ylenv[i], dtab[x.table], table_len[x.table]});
       yptr[x.child_h] = yptr[i] + (x.n - nodes[x.child_h].n);
       yptr[x.child_l] = C + (x.n - nodes[x.child_l].n);
     }
@@ -1439,6 +1424,129 @@ int radix_tree_locked(const uint32_t *y, size_t ylen, const bc_radix_node *nodes
   if ((r = stage_d2h((const char *)(dsd + s_off[0]), jobs, nodes[0].k * 4))) return r;
   CK(cudaStreamSynchronize(g.stream));
   return BC_OK;
+}
+
+// Host fraction and host table entries: both cross once, then the core.
+int radix_tree_locked(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nn,
+                      const uint32_t *const *table, const size_t *table_len, int ntable, double alpha,
+                      uint32_t *out) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (!y || !ylen || !nodes || !nn || !out || (ntable && (!table || !table_len))) return fail(BC_ERR_INVALID);
+  size_t tab_total = 0;
+  std::vector<size_t> tab_off(ntable);
+  for (int t = 0; t < ntable; t++) {
+    tab_off[t] = tab_total;
+    tab_total += (table_len[t] + 63) & ~size_t(63);
+  }
+  const size_t ypad = (ylen + 63) & ~size_t(63);
+  DevBuf din;
+  int r;
+  if ((r = din.alloc((ypad + tab_total) * 4))) return r;
+  uint32_t *dy = (uint32_t *)din.p;
+  std::vector<SpanJob> jobs;
+  jobs.push_back({0, (char *)y, ylen * 4});
+  for (int t = 0; t < ntable; t++)
+    if (table_len[t]) jobs.push_back({(ypad + tab_off[t]) * 4, (char *)table[t], table_len[t] * 4});
+  if ((r = stage_h2d((char *)din.p, jobs, (ypad + tab_total) * 4))) return r;
+  std::vector<const uint32_t *> dtab(ntable);
+  for (int t = 0; t < ntable; t++) dtab[t] = dy + ypad + tab_off[t];
+  return radix_tree_core(dy, ylen, nodes, nn, dtab.data(), table_len, ntable, alpha, out);
+}
+
+// Significant length of a product of CL limbs under the reference's trimming
+// (bigfloat/mul.c:664-675): one top zero limb dropped, then, above 1000
+// limbs, every top zero limb.
+int trimmed_len(const uint32_t *dC, size_t CL, size_t *len) {
+  size_t n = CL;
+  uint32_t top[8];
+  size_t have = 0, base = 0;  // top[] holds limbs [base, base + have)
+  auto limb = [&](size_t i, uint32_t *v) -> int {
+    if (i < base || i >= base + have) {
+      have = std::min<size_t>(8, i + 1);
+      base = i + 1 - have;
+      CK(cudaMemcpyAsync(top, dC + base, have * 4, cudaMemcpyDeviceToHost, g.stream));
+      CK(cudaStreamSynchronize(g.stream));
+    }
+    *v = top[i - base];
+    return BC_OK;
+  };
+  uint32_t v = 0;
+  int r;
+  if (n && ((r = limb(n - 1, &v)))) return r;
+  if (n && v == 0) n--;
+  if (n > 1000)
+    while (n > 0) {
+      if ((r = limb(n - 1, &v))) return r;
+      if (v) break;
+      n--;
+    }
+  *len = n;
+  return BC_OK;
+}
+
+// The power table of the conversion built in device memory: entry 0 comes
+// from the host; entry i from entry steps[i].src < i by the step the
+// reference's table construction takes (bigfloat/radix.c:156-205): times
+// 10^9 (len + 1 limbs, untrimmed), a squaring (trimmed product), or a
+// squaring then times 10^9 (trimmed square plus one limb).  The products
+// are the library's own exact products on device operands.
+int radix_tree_pow_locked(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nn, const uint32_t *t0,
+                          size_t t0len, const bc_radix_pow_step *steps, int ntable, double alpha, uint32_t *out) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (!y || !ylen || !nodes || !nn || !out || ntable < 1 || !t0 || !t0len || !steps) return fail(BC_ERR_INVALID);
+  for (int i = 1; i < ntable; i++)
+    if (steps[i].src < 0 || steps[i].src >= i || steps[i].op < 1 || steps[i].op > 3) return fail(BC_ERR_INVALID);
+  std::vector<DevBuf> tab(ntable + 1);  // the last one holds y and 10^9
+  std::vector<size_t> tlen(ntable);
+  std::vector<const uint32_t *> dtab(ntable);
+  int r;
+  const size_t ypad = (ylen + 63) & ~size_t(63);
+  if ((r = tab[ntable].alloc((ypad + 64) * 4))) return r;
+  uint32_t *dy = (uint32_t *)tab[ntable].p, *dbase = dy + ypad;
+  {
+    std::vector<SpanJob> jobs{{0, (char *)y, ylen * 4}};
+    if ((r = stage_h2d((char *)dy, jobs, ylen * 4))) return r;
+    const uint32_t nine = DEC_BASE;
+    CK(cudaMemcpyAsync(dbase, &nine, 4, cudaMemcpyHostToDevice, g.stream));
+  }
+  if ((r = tab[0].alloc(t0len * 4))) return r;
+  CK(cudaMemcpyAsync(tab[0].p, t0, t0len * 4, cudaMemcpyHostToDevice, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  tlen[0] = t0len;
+  dtab[0] = (const uint32_t *)tab[0].p;
+  bc_batch_stats st{};
+  for (int i = 1; i < ntable; i++) {
+    const int j = steps[i].src, op = steps[i].op;
+    const uint32_t *X = dtab[j];
+    const size_t XL = tlen[j];
+    if (op == 1) {  // times 10^9
+      const size_t CL = XL + 1;
+      if ((r = tab[i].alloc(CL * 4))) return r;
+      bc_mul_desc d{(uint32_t *)tab[i].p, CL, X, XL, dbase, 1};
+      if ((r = mul_batch_locked(&d, 1, &st, nullptr, BC_BATCH_DEVICE_OPERANDS))) return r;
+      tlen[i] = CL;
+    } else {
+      const size_t CL = 2 * XL;
+      DevBuf sq;
+      if ((r = sq.alloc(CL * 4))) return r;
+      bc_mul_desc d{(uint32_t *)sq.p, CL, X, XL, X, XL};
+      if ((r = mul_batch_locked(&d, 1, &st, nullptr, BC_BATCH_DEVICE_OPERANDS))) return r;
+      size_t L = 0;
+      if ((r = trimmed_len((const uint32_t *)sq.p, CL, &L))) return r;
+      if (op == 2) {
+        tab[i].p = sq.p;
+        sq.p = nullptr;
+        tlen[i] = L;
+      } else {  // then times 10^9 into L + 1 limbs
+        if ((r = tab[i].alloc((L + 1) * 4))) return r;
+        bc_mul_desc d2{(uint32_t *)tab[i].p, L + 1, (const uint32_t *)sq.p, L, dbase, 1};
+        if ((r = mul_batch_locked(&d2, 1, &st, nullptr, BC_BATCH_DEVICE_OPERANDS))) return r;
+        tlen[i] = L + 1;
+      }
+    }
+    dtab[i] = (const uint32_t *)tab[i].p;
+  }
+  return radix_tree_core(dy, ylen, nodes, nn, dtab.data(), tlen.data(), ntable, alpha, out);
 }
 
 int e_series_locked(uint32_t a, uint32_t b, uint32_t **hP, size_t *PL, uint32_t **hQ, size_t *QL,
@@ -1723,6 +1831,13 @@ int bc_gpu_radix_tree(const uint32_t *y, size_t ylen, const bc_radix_node *nodes
                       uint32_t *out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   return radix_tree_locked(y, ylen, nodes, nnodes, table, table_len, ntable, alpha, out);
+}
+
+int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nnodes,
+                          const uint32_t *t0, size_t t0len, const bc_radix_pow_step *steps, int ntable, double alpha,
+                          uint32_t *out) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return radix_tree_pow_locked(y, ylen, nodes, nnodes, t0, t0len, steps, ntable, alpha, out);
 }
 
 int bc_gpu_radix_leaves(const bc_radix_leaf *leaves, size_t count, double alpha) {

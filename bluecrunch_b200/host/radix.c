@@ -162,6 +162,45 @@ static void table_build(pow_table *tb, size_t k) {
   }
 }
 
+/* The same table as a plan for the device: exponents, entry 0's value, and
+ * for every later entry the step table_build would take (op 1: times 10^9
+ * from entry e-1; op 2: square of entry e/2; op 3: that square times 10^9). */
+static void table_plan(pow_table *tb, size_t k, bc_radix_pow_step *steps) {
+  memset(tb->exps, 0, sizeof tb->exps);
+  tb->n = 0;
+  if (k < KT) return;
+  table_collect(tb, k);
+  int n = 0;
+  while (n < TABLE_SLOTS && tb->exps[n]) n++;
+  qsort(tb->exps, (size_t)n, sizeof(size_t), cmp_size);
+  tb->n = n;
+  for (int i = 0; i < n; i++) bigfloat_new(tb->val[i]);
+  bigfloat_t base;
+  bigfloat_new(base);
+  bigfloat_set(base, NEWBASE);
+  bigfloat_exp(tb->val[0], base, tb->exps[0]);
+  bigfloat_free(base);
+  steps[0].src = 0;
+  steps[0].op = 0;
+  for (int i = 1; i < n; i++) {
+    size_t e = tb->exps[i];
+    int j = table_find(tb, e - 1);
+    if (j >= 0 && j < i) {
+      steps[i].src = j;
+      steps[i].op = 1;
+      continue;
+    }
+    j = table_find(tb, e / 2);
+    if (j >= 0 && j < i) {
+      steps[i].src = j;
+      steps[i].op = (e & 1) ? 3 : 2;
+      continue;
+    }
+    fprintf(stderr, "radix table: no predecessor for 10^(9*%zu)\n", e);
+    abort();
+  }
+}
+
 static void table_free(pow_table *tb) {
   for (int i = 0; i < tb->n; i++) bigfloat_free(tb->val[i]);
   tb->n = 0;
@@ -389,8 +428,11 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
 /* ---------------------------------------------------------------- tree on the device */
 
 /* The same tree planned here (split_sizes, power-table entries) and run in
- * one call, bc_gpu_radix_tree, with every product, leaf and merge in device
- * memory: the fraction and the table go over once, the digits come back once. */
+ * one call, bc_gpu_radix_tree_pow, with the power table built from its plan
+ * and every product, leaf and merge in device memory: the fraction and the
+ * table's first entry go over once, the digits come back once. */
+static bc_radix_pow_step g_steps[TABLE_SLOTS];
+
 static void convert_tree(bigfloat_t target, size_t k0, const _bigfloat_struct *y0, size_t n0, size_t g) {
   double t0 = wall_now();
   size_t cap = 64, nn = 1;
@@ -416,22 +458,20 @@ static void convert_tree(bigfloat_t target, size_t k0, const _bigfloat_struct *y
     nd[nn++] = h;
     nd[nn++] = l;
   }
-  const uint32_t **tab = (const uint32_t **)bc_xmalloc((size_t)(g_tab.n ? g_tab.n : 1) * sizeof(uint32_t *));
-  size_t *tlen = (size_t *)bc_xmalloc((size_t)(g_tab.n ? g_tab.n : 1) * sizeof(size_t));
-  for (int t = 0; t < g_tab.n; t++) {
-    tab[t] = g_tab.val[t]->coef;
-    tlen[t] = g_tab.val[t]->len;
-  }
   bigfloat_alloc(target, k0);
   bc_host_ensure_gpu();
-  int rc = bc_gpu_radix_tree(y0->coef, y0->len, nd, nn, tab, tlen, g_tab.n, ALPHA, target->coef);
+  int rc;
+  if (g_tab.n > 0) {
+    rc = bc_gpu_radix_tree_pow(y0->coef, y0->len, nd, nn, g_tab.val[0]->coef, g_tab.val[0]->len, g_steps, g_tab.n,
+                               ALPHA, target->coef);
+  } else {
+    rc = bc_gpu_radix_tree(y0->coef, y0->len, nd, nn, NULL, NULL, 0, ALPHA, target->coef);
+  }
   if (rc != BC_OK) {
     fprintf(stderr, "bigfloat_radix: GPU conversion tree of %zu nodes failed: %s\n", nn, bc_gpu_strerror(rc));
     abort();
   }
   if (getenv("BC_STATS")) printf("    conversion: %zu nodes on the device, %.3f s\n", nn, wall_now() - t0);
-  free(tab);
-  free(tlen);
   free(nd);
 }
 
@@ -445,8 +485,10 @@ void bigfloat_radix(bigfloat_t target, const bigfloat_t a) {
   size_t k = (size_t)ceil((double)n * LOGR) - 1;
   double gd = ceil(log((double)k) / log(OLDBASE)) + 1;
   size_t g = (size_t)(gd > KT ? gd : KT);
+  const int tree = !getenv("BC_RADIX_PERCALL") && !getenv("BC_RADIX_LEVELS");
   task_start(2, "Precomputing base conversion table");
-  table_build(&g_tab, k);
+  if (tree) table_plan(&g_tab, k, g_steps); /* the tree builds the rest on the device */
+  else table_build(&g_tab, k);
   task_end(2);
   bigfloat_alloc(target, k);
   task_start(2, "Conversion");

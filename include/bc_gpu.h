@@ -149,6 +149,20 @@ int bc_gpu_radix_tree(const uint32_t *y, size_t ylen, const bc_radix_node *nodes
                       const uint32_t *const *table, const size_t *table_len, int ntable, double alpha,
                       uint32_t *out);
 
+/* Same tree with the power table built in device memory: entry 0 is t0
+ * (t0len limbs, host); entry i >= 1 comes from entry steps[i].src (< i) by
+ * op 1 = times 10^9 (src length + 1 limbs), op 2 = squaring (product
+ * trimmed as bigfloat_mul trims it), op 3 = squaring then times 10^9 (trimmed
+ * square plus one limb) — the steps of the reference's table construction
+ * (bigfloat/radix.c:156-205).  Only y, t0 and the digits cross the bus. */
+typedef struct {
+  int src;
+  int op;
+} bc_radix_pow_step;
+int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nnodes,
+                          const uint32_t *t0, size_t t0len, const bc_radix_pow_step *steps, int ntable, double alpha,
+                          uint32_t *out);
+
 /* Launch on this CUDA stream (cudaStream_t as void*; NULL = library stream).
  * Calls still return only when their results are complete. */
 int bc_gpu_set_stream(void *stream);
