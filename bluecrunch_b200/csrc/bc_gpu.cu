@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -28,6 +29,7 @@
 #include "bc_bsr.cuh"
 #include "bc_radix.cuh"
 #include "bc_rows_warp.cuh"
+#include "bc_arith.cuh"
 
 using namespace bc;
 
@@ -1549,6 +1551,262 @@ int radix_tree_pow_locked(const uint32_t *y, size_t ylen, const bc_radix_node *n
   return radix_tree_core(dy, ylen, nodes, nn, dtab.data(), tlen.data(), ntable, alpha, out);
 }
 
+// ------------------------------------------------------------------ Newton iteration in device memory
+// Bigfloats held in device memory (value = sign * sum p[i] 2^(32(i+exp)),
+// sign 1 positive, 0 negative, len 0 for zero), and the operations the
+// reciprocal's Newton step uses, each with the semantics of the host library
+// (bigfloat/mul.c:555-676, bigfloat/addsub.c:33-237) so the values are the
+// same limb for limb.
+struct DNum {
+  std::shared_ptr<DevBuf> own;
+  const uint32_t *p = nullptr;
+  size_t len = 0;
+  long long exp = 0;
+  int sign = 1;
+};
+
+int dnum_alloc(DNum &x, size_t limbs) {
+  x.own = std::make_shared<DevBuf>();
+  int r = x.own->alloc(std::max<size_t>(limbs, 1) * 4);
+  if (r) return r;
+  x.p = (const uint32_t *)x.own->p;
+  return BC_OK;
+}
+
+int dnum_upload(DNum &x, const bc_bignum &h) {
+  x = DNum();
+  x.len = h.len;
+  x.exp = h.exp;
+  x.sign = h.sign;
+  if (!h.len) return BC_OK;
+  int r = dnum_alloc(x, h.len);
+  if (r) return r;
+  std::vector<SpanJob> jobs{{0, (char *)h.coef, h.len * 4}};
+  return stage_h2d((char *)x.own->p, jobs, h.len * 4);
+}
+
+// bigfloat_mul: operands chopped to their top p+2 limbs (all limbs when
+// p = 0), the exact product, its top zero limb dropped (above 1000 limbs
+// every top zero limb).
+int dnum_mul(DNum &t, const DNum &a, const DNum &b, size_t p) {
+  if (!a.len || !b.len) {
+    t = DNum();
+    return BC_OK;
+  }
+  const size_t pp = p == 0 ? a.len + b.len : p + 2;
+  const uint32_t *A = a.p, *B = b.p;
+  size_t AL = a.len, BL = b.len;
+  long long ea = a.exp, eb = b.exp;
+  if (AL > pp) { A += AL - pp; ea += (long long)(AL - pp); AL = pp; }
+  if (BL > pp) { B += BL - pp; eb += (long long)(BL - pp); BL = pp; }
+  DNum c;
+  const size_t CL = AL + BL;
+  int r;
+  if ((r = dnum_alloc(c, CL))) return r;
+  bc_mul_desc d{(uint32_t *)c.p, CL, A, AL, B, BL};
+  bc_batch_stats st{};
+  if ((r = mul_batch_locked(&d, 1, &st, nullptr, BC_BATCH_DEVICE_OPERANDS))) return r;
+  if ((r = trimmed_len(c.p, CL, &c.len))) return r;
+  c.exp = ea + eb;
+  c.sign = a.sign == b.sign;
+  t = c;
+  return BC_OK;
+}
+
+// The window [bot, top) of a sum or difference at precision p and the
+// exponent the reference gives its result (top - p, p the window length when
+// untruncated).
+void dnum_window(const DNum &a, const DNum &b, size_t p, long long *bot, long long *top, long long *e) {
+  const long long ta = a.exp + (long long)a.len, tb = b.exp + (long long)b.len;
+  *top = std::max(ta, tb);
+  *bot = std::min(a.exp, b.exp);
+  const long long tl = *top - *bot;
+  const long long pp = p == 0 ? tl : (long long)p + 2;
+  if (tl > pp) *bot = *top - pp;
+  *e = *top - pp;
+}
+
+WinOp win_of(const DNum &x, long long bot, long long n) {
+  WinOp w;
+  w.x = x.p;
+  w.lo = x.exp - bot;
+  w.hi = x.len ? std::min(x.exp + (long long)x.len - bot, n) : w.lo;
+  return w;
+}
+
+// _bigfloat_uadd / _bigfloat_usub: the window's limbs of a + b or a - b
+// (|a| >= |b| assumed by the caller), sign of a; a sum keeps a carry limb, a
+// difference drops its top zero limbs (zero when none is left).
+int dnum_uaddsub(DNum &t, const DNum &a, const DNum &b, size_t p, bool sub) {
+  long long bot, top, e;
+  dnum_window(a, b, p, &bot, &top, &e);
+  const long long n = top - bot;
+  DNum c;
+  int r;
+  if ((r = dnum_alloc(c, (size_t)n + 1))) return r;
+  const unsigned long long tiles = ((unsigned long long)n + ADD_TILE - 1) / ADD_TILE;
+  DevBuf scratch;
+  const size_t o_st = 256, o_top = o_st + align256(tiles * 4);
+  if ((r = scratch.alloc(o_top + 256))) return r;
+  char *sp = (char *)scratch.p;
+  CK(cudaMemsetAsync(sp, 0, o_top + 256, g.stream));
+  AddSubParams ap;
+  ap.a = win_of(a, bot, n);
+  ap.b = win_of(b, bot, n);
+  ap.r = (uint32_t *)c.p;
+  ap.n = (unsigned long long)n;
+  ap.sub = sub ? 1 : 0;
+  ap.tiles = tiles;
+  ap.counter = (unsigned int *)sp;
+  ap.cout = (unsigned int *)(sp + 4);
+  ap.flags = (unsigned int *)(sp + 8);
+  ap.status = (uint32_t *)(sp + o_st);
+  if (n > 0) {
+    const unsigned grid = (unsigned)std::min<unsigned long long>(tiles, (unsigned long long)g.sm_count * 8);
+    k_addsub_win<<<grid, ADD_NT, 0, g.stream>>>(ap);
+    CK(cudaGetLastError());
+  }
+  unsigned long long len = (unsigned long long)n;
+  if (sub && n > 0) {
+    unsigned long long *dtop = (unsigned long long *)(sp + o_top);
+    const unsigned grid = (unsigned)std::min<unsigned long long>(((unsigned long long)n + 255) / 256,
+                                                                 (unsigned long long)g.sm_count * 8);
+    k_top_nonzero<<<grid, 256, 0, g.stream>>>(c.p, (unsigned long long)n, dtop);
+    CK(cudaGetLastError());
+  }
+  unsigned int head[4];
+  unsigned long long toplen = 0;
+  CK(cudaMemcpyAsync(head, sp, 16, cudaMemcpyDeviceToHost, g.stream));
+  if (sub && n > 0) CK(cudaMemcpyAsync(&toplen, sp + o_top, 8, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  if (head[2]) return fail(BC_ERR_TIMEOUT);
+  if (sub) {
+    len = toplen;
+  } else if (head[1]) {
+    const uint32_t one = 1;
+    CK(cudaMemcpyAsync((uint32_t *)c.p + n, &one, 4, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    len = (unsigned long long)n + 1;
+  }
+  if (len == 0) {
+    t = DNum();
+    return BC_OK;
+  }
+  c.len = (size_t)len;
+  c.exp = e;
+  c.sign = a.sign;
+  t = c;
+  return BC_OK;
+}
+
+// Compare |a| and |b| (bigfloat/addsub.c:33-63): 1, -1 or 0.
+int dnum_ucmp(const DNum &a, const DNum &b, int *res) {
+  const long long ta = a.exp + (long long)a.len, tb = b.exp + (long long)b.len;
+  if (ta != tb) {
+    *res = ta > tb ? 1 : -1;
+    return BC_OK;
+  }
+  const long long lo = std::min(a.exp, b.exp), n = ta - lo + 1;
+  const WinOp wa = win_of(a, lo, n), wb = win_of(b, lo, n);
+  DevBuf scratch;
+  int r;
+  if ((r = scratch.alloc(256))) return r;
+  unsigned long long *dhi = (unsigned long long *)scratch.p;
+  CK(cudaMemsetAsync(dhi, 0, 8, g.stream));
+  if (n > 0) {
+    const unsigned grid =
+        (unsigned)std::min<unsigned long long>(((unsigned long long)n + 255) / 256, (unsigned long long)g.sm_count * 8);
+    k_first_diff<<<grid, 256, 0, g.stream>>>(wa, wb, (unsigned long long)n, dhi);
+    CK(cudaGetLastError());
+  }
+  unsigned long long hi = 0;
+  CK(cudaMemcpyAsync(&hi, dhi, 8, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  if (!hi) {
+    *res = 0;
+    return BC_OK;
+  }
+  const long long i = (long long)hi - 1;
+  uint32_t x = 0, y = 0;
+  if (i >= wa.lo && i < wa.hi) CK(cudaMemcpy(&x, wa.x + (i - wa.lo), 4, cudaMemcpyDeviceToHost));
+  if (i >= wb.lo && i < wb.hi) CK(cudaMemcpy(&y, wb.x + (i - wb.lo), 4, cudaMemcpyDeviceToHost));
+  *res = x > y ? 1 : -1;
+  return BC_OK;
+}
+
+void dnum_neg(DNum &t) {
+  if (t.len) t.sign = !t.sign;
+}
+
+// bigfloat_sub (bigfloat/addsub.c:212-237).
+int dnum_sub(DNum &t, const DNum &a, const DNum &b, size_t p) {
+  if (a.sign != b.sign) return dnum_uaddsub(t, a, b, p, false);
+  int c = 0, r;
+  if ((r = dnum_ucmp(a, b, &c))) return r;
+  if (c > 0) return dnum_uaddsub(t, a, b, p, true);
+  if ((r = dnum_uaddsub(t, b, a, p, true))) return r;
+  dnum_neg(t);
+  return BC_OK;
+}
+
+// The reciprocal's Newton levels (bigfloat/rcp.c:15-101) from r0 upward,
+// levels[k] the precision of level k in increasing order:
+//   r <- r - (r*x - 1)*r, each product and difference at that precision;
+// then the quotient num * r at precision pdiv when num is given.
+int newton_locked(const bc_bignum *den, const bc_bignum *r0, const size_t *levels, int nlev, const bc_bignum *num,
+                  size_t pdiv, bc_bignum_out *out) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (!den || !r0 || !out || nlev < 0 || (nlev && !levels)) return fail(BC_ERR_INVALID);
+  const bool stats = getenv("BC_STATS") != nullptr;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto secs = [](std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  };
+  int r;
+  DNum D, R, N, one;
+  auto t0 = now();
+  if ((r = dnum_upload(D, *den)) || (r = dnum_upload(R, *r0))) return r;
+  if (num && (r = dnum_upload(N, *num))) return r;
+  {
+    const uint32_t v = 1;
+    bc_bignum h{&v, 1, 0, 1};
+    if ((r = dnum_upload(one, h))) return r;
+  }
+  if (stats) fprintf(stderr, "      newton on the device: operands up %.3f s\n", secs(t0));
+  for (int k = 0; k < nlev; k++) {
+    const size_t p = levels[k];
+    t0 = now();
+    DNum ax, err, corr, next;
+    if ((r = dnum_mul(ax, D, R, p)) || (r = dnum_sub(err, ax, one, p)) || (r = dnum_mul(corr, err, R, p)) ||
+        (r = dnum_sub(next, R, corr, p)))
+      return r;
+    R = next;
+    if (stats) fprintf(stderr, "      newton level p=%zu on the device: %.3f s\n", p, secs(t0));
+  }
+  DNum T = R;
+  if (num) {
+    t0 = now();
+    if ((r = dnum_mul(T, N, R, pdiv))) return r;
+    if (stats) fprintf(stderr, "      quotient on the device: %.3f s\n", secs(t0));
+  }
+  out->coef = nullptr;
+  out->len = T.len;
+  out->exp = T.exp;
+  out->sign = T.sign;
+  if (T.len) {
+    out->coef = (uint32_t *)malloc(T.len * 4);
+    if (!out->coef) return fail(BC_ERR_NOMEM);
+    std::vector<SpanJob> jobs{{0, (char *)out->coef, T.len * 4}};
+    if ((r = stage_d2h((const char *)T.p, jobs, T.len * 4))) {
+      free(out->coef);
+      out->coef = nullptr;
+      return r;
+    }
+    CK(cudaStreamSynchronize(g.stream));
+  }
+  return BC_OK;
+}
+
 int e_series_locked(uint32_t a, uint32_t b, uint32_t **hP, size_t *PL, uint32_t **hQ, size_t *QL,
                     bc_batch_stats *st) {
   if (!g.init) return fail(BC_ERR_NOT_INIT);
@@ -1838,6 +2096,12 @@ int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *n
                           uint32_t *out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   return radix_tree_pow_locked(y, ylen, nodes, nnodes, t0, t0len, steps, ntable, alpha, out);
+}
+
+int bc_gpu_newton(const bc_bignum *den, const bc_bignum *r0, const size_t *levels, int nlevels, const bc_bignum *num,
+                  size_t pdiv, bc_bignum_out *out) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return newton_locked(den, r0, levels, nlevels, num, pdiv, out);
 }
 
 int bc_gpu_radix_leaves(const bc_radix_leaf *leaves, size_t count, double alpha) {

@@ -13,6 +13,7 @@
 #include <stdlib.h>
 #include <time.h>
 
+#include "bc_gpu.h"
 #include "bc_host.h"
 #include "bigfloat.h"
 
@@ -50,18 +51,58 @@ static void seed(bigfloat_t t, const bigfloat_t a) {
   t->exp = e;
 }
 
+/* Precision of the level below p (bigfloat/rcp.c:73-80). */
+static size_t rcp_inner(size_t p) { return p == 1 ? 0 : (p == 2 ? 1 : p / 2 + 1); }
+
+/* Levels of BC_DEVICE_NEWTON limbs and more run in device memory
+ * (bc_gpu_newton): the host computes the reciprocal at the first level below
+ * that, the device the levels above it and, for a division, the quotient.
+ * $BC_NEWTON_HOST keeps every level on the host.  Returns 1 when done. */
+#define BC_DEVICE_NEWTON ((size_t)1 << 16)
+static int newton_device(bigfloat_t t, const bigfloat_t num, const bigfloat_t den, size_t p, size_t pdiv) {
+  if (p < BC_DEVICE_NEWTON || getenv("BC_NEWTON_HOST")) return 0;
+  size_t lv[64];
+  int n = 0;
+  size_t q = p;
+  while (q >= BC_DEVICE_NEWTON && n < 64) {
+    lv[n++] = q;
+    q = rcp_inner(q);
+  }
+  /* lv[0] = p > lv[1] > ... > lv[n-1] >= BC_DEVICE_NEWTON > q */
+  bigfloat_t r0;
+  bigfloat_new(r0);
+  bigfloat_rcp(r0, den, q);
+  size_t up[64];
+  for (int k = 0; k < n; k++) up[k] = lv[n - 1 - k];
+  bc_bignum d = {den->coef, den->len, den->exp, den->sign}, r = {r0->coef, r0->len, r0->exp, r0->sign};
+  bc_bignum a = {num ? num->coef : NULL, num ? num->len : 0, num ? num->exp : 0, num ? num->sign : 1};
+  bc_bignum_out out;
+  bc_host_ensure_gpu();
+  const int rc = bc_gpu_newton(&d, &r, up, n, num ? &a : NULL, pdiv, &out);
+  bigfloat_free(r0);
+  if (rc != BC_OK) {
+    fprintf(stderr, "bluecrunch: Newton iteration on the GPU failed: %s\n", bc_gpu_strerror(rc));
+    abort();
+  }
+  free(t->coef);
+  t->coef = out.coef;
+  t->len = out.len;
+  t->exp = out.exp;
+  t->sign = out.sign;
+  return 1;
+}
+
 void bigfloat_rcp(bigfloat_t t, const bigfloat_t a, size_t p) {
   if (a->len == 0) {
     fprintf(stderr, "Divide by Zero\n");
     abort();
   }
+  if (newton_device(t, NULL, a, p, 0)) return;
   if (p == 0) {
     seed(t, a);
     return;
   }
-  size_t s = p / 2 + 1;
-  if (p == 1) s = 0;
-  if (p == 2) s = 1;
+  const size_t s = rcp_inner(p);
   bigfloat_t r, one, ax, err, corr;
   bigfloat_new(r);
   bigfloat_new(one);
@@ -93,6 +134,10 @@ void bigfloat_div(bigfloat_t t, const bigfloat_t a, const bigfloat_t b, size_t p
   bigfloat_t r;
   bigfloat_new(r);
   if (p == 0) p = a->len + b->len;
+  if (b->len && newton_device(t, a, b, p, p)) {
+    bigfloat_free(r);
+    return;
+  }
   bigfloat_rcp(r, b, p);
   const double t0 = now_s();
   bigfloat_mul(t, a, r, p);

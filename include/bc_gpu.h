@@ -159,6 +159,31 @@ typedef struct {
   int src;
   int op;
 } bc_radix_pow_step;
+/* A bigfloat as the host library holds it (include/bigfloat.h): value =
+ * +-sum coef[i] 2^(32(i+exp)), sign 1 positive, 0 negative, len 0 for zero. */
+typedef struct {
+  const uint32_t *coef;
+  size_t len;
+  int64_t exp;
+  int sign;
+} bc_bignum;
+typedef struct {
+  uint32_t *coef; /* malloc'd (the caller frees it); NULL when len == 0 */
+  size_t len;
+  int64_t exp;
+  int sign;
+} bc_bignum_out;
+
+/* The upper levels of the reciprocal's Newton iteration (bigfloat/rcp.c:15-101)
+ * in device memory: from r0 (the reciprocal of den at the lowest of these
+ * levels' predecessor precision), for each precision levels[0] <
+ * levels[1] < ...:  r <- r - (r*den - 1)*r, every product and difference
+ * with the host library's semantics at that precision; then, when num is not
+ * NULL, the quotient num*r at precision pdiv (bigfloat/div.c:14-27).  Only
+ * den, num, r0 and the result cross the bus. */
+int bc_gpu_newton(const bc_bignum *den, const bc_bignum *r0, const size_t *levels, int nlevels, const bc_bignum *num,
+                  size_t pdiv, bc_bignum_out *out);
+
 int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nnodes,
                           const uint32_t *t0, size_t t0len, const bc_radix_pow_step *steps, int ntable, double alpha,
                           uint32_t *out);
