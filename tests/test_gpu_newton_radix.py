@@ -104,3 +104,46 @@ def test_fifty_million_digits_verified():
                        text=True, timeout=900)
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip().splitlines()[-1].startswith("OK"), p.stdout[-2000:]
+
+
+_DEV_VS_HOST = r"""
+import sys, hashlib, os
+sys.path.insert(0, {root!r}); sys.path.insert(0, {golden!r})
+from bluecrunch_b200.bigfloat import Lib, limbs
+import oracle
+lib = Lib()
+out = []
+for seed, n, p, e in {cases!r}:
+    xl = oracle.random_limbs(seed, n); xl[-1] |= 1
+    yl = oracle.random_limbs(seed ^ 0x77, n + 3)
+    x = lib.make(xl, exp=e); y = lib.make(yl, exp=-(n + 3) // 2)
+    r, q = lib.make(), lib.make()
+    lib.rcp(r, x, p)
+    lib.div(q, y, x, p)
+    for z in (r, q):
+        out.append((int(z.exp), int(z.len), int(z.sign), hashlib.sha256(limbs(z).astype("<u4").tobytes()).hexdigest()))
+    for z in (x, y, r, q):
+        lib.free(z)
+print(repr(out))
+"""
+
+
+def test_device_newton_matches_host_newton():
+    # the Newton levels of 2^16 limbs and more run in device memory
+    # (bc_gpu_newton); BC_NEWTON_HOST=1 runs every level through the host
+    # library: both must give the same limbs, exponent and sign, for
+    # reciprocals and quotients of assorted sizes, precisions and exponents
+    import subprocess
+    cases = [(11, 70_000, 66_000, -69_999), (12, 300_000, 300_000, -5), (13, 150_000, 400_000, 3),
+             (14, 1_000_000, 700_000, -1_000_000)]
+    code = _DEV_VS_HOST.format(root=ROOT, golden=os.path.join(ROOT, "tests", "golden"), cases=cases)
+    res = []
+    for host in (False, True):
+        env = dict(os.environ)
+        env.pop("BC_NEWTON_HOST", None)
+        if host:
+            env["BC_NEWTON_HOST"] = "1"
+        p = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=900)
+        assert p.returncode == 0, p.stderr[-2000:]
+        res.append(p.stdout.strip().splitlines()[-1])
+    assert res[0] == res[1]
