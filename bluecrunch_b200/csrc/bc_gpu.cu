@@ -124,6 +124,10 @@ struct Ctx {
   int last_cuda = 0;
   bool time_kernels = false;
   bool rows_warp = true;  // 1024-point rows by k2_rows_w1024 ($BC_ROWS_WARP=0: the block kernel)
+  // second operand's copy of a single product from pinned host memory: on
+  // copy_stream, so the outer pass packs the first operand meanwhile
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ev[2] = {nullptr, nullptr};
   std::vector<std::pair<const char *, double>> ktimes;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;
@@ -567,7 +571,8 @@ bool shape_launch_ok(const Shape &s, bool sq) {
 // i*M).  Scratch (records, lookback status, counter) must be set up and the
 // counter and status words zeroed by the caller.
 int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, unsigned long long carry_tiles,
-                 double2 *slabA, double2 *slabB, cudaStream_t stream, bool timed, size_t *nl) {
+                 double2 *slabA, double2 *slabB, cudaStream_t stream, bool timed, size_t *nl,
+                 cudaEvent_t b_ready = nullptr) {
   int r;
   if (!shape_launch_ok(s, sq)) return fail(BC_ERR_INVALID);
   if (s.levels == 1) return launch(get_small(s.M, sq), n, p, nl, stream, timed);
@@ -575,7 +580,19 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
   KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
   const int W1 = ko.threads / (s.L1 / PTS);
   const int nops = sq ? 1 : 2;
-  if ((r = launch(ko, n * nops * (long long)(S1 / W1), p, nl, stream, timed))) return r;
+  if (b_ready && !sq) {
+    // operand A is on the device, B still crossing: pack A, then wait for B
+    ClassParams pa = p, pb = p;
+    pa.op0 = 0;
+    pa.nops_fwd = 1;
+    pb.op0 = 1;
+    pb.nops_fwd = 1;
+    if ((r = launch(ko, n * (long long)(S1 / W1), pa, nl, stream, timed))) return r;
+    CK(cudaStreamWaitEvent(stream, b_ready, 0));
+    if ((r = launch(ko, n * (long long)(S1 / W1), pb, nl, stream, timed))) return r;
+  } else if ((r = launch(ko, n * nops * (long long)(S1 / W1), p, nl, stream, timed))) {
+    return r;
+  }
   CUtensorMap midA, midB;
   if (s.levels == 3) {
     const cuuint64_t dims[4] = {2 * Lr, (cuuint64_t)s.L2, (cuuint64_t)s.L1, (cuuint64_t)n};
@@ -987,6 +1004,7 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     st->h2d_bytes += stage_in;
     g_prof.bytes_in += stage_in;
   }
+  bool b_late = false;  // B of the single product arrives on the copy stream
   for (size_t i = 0; i < nw; i++) {
     const bc_mul_desc &d = items[works[i]->idx];
     const Plan &pl = works[i]->pl;
@@ -1002,7 +1020,21 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     else if (pin_inB_off[i] != SIZE_MAX) runs[i].dB = (const uint32_t *)(base + off_stage_in + pin_inB_off[i]);
     else {
       runs[i].dB = (const uint32_t *)(base + slots[i].off_dB);
-      CK(cudaMemcpyAsync((void *)runs[i].dB, d.B, pl.BL * 4, cudaMemcpyHostToDevice, g.stream));
+      if (nw == 1 && pl.shape.levels >= 2 && pl.BL >= ((size_t)1 << 20)) {
+        // a single large product: B crosses on the copy stream (after the
+        // library stream's earlier work, which may still read this slot)
+        // while the outer pass packs A
+        if (!g.copy_stream) CK(cudaStreamCreateWithFlags(&g.copy_stream, cudaStreamNonBlocking));
+        for (auto &e : g.copy_ev)
+          if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        CK(cudaEventRecord(g.copy_ev[0], g.stream));
+        CK(cudaStreamWaitEvent(g.copy_stream, g.copy_ev[0], 0));
+        CK(cudaMemcpyAsync((void *)runs[i].dB, d.B, pl.BL * 4, cudaMemcpyHostToDevice, g.copy_stream));
+        CK(cudaEventRecord(g.copy_ev[1], g.copy_stream));
+        b_late = true;
+      } else {
+        CK(cudaMemcpyAsync((void *)runs[i].dB, d.B, pl.BL * 4, cudaMemcpyHostToDevice, g.stream));
+      }
       st->h2d_bytes += pl.BL * 4;
     }
     if (pin_out_off[i] != SIZE_MAX) runs[i].dC = (uint32_t *)(base + off_stage_out + pin_out_off[i]);
@@ -1080,7 +1112,8 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     p.carry_tiles = tiles;
     const ClassSlab &cs = slab[c.first];
     if ((r = launch_class(s, sq, p, (long long)n, tiles, (double2 *)(base + cs.offA),
-                          sq ? nullptr : (double2 *)(base + cs.offB), g.stream, true, &st->launches)))
+                          sq ? nullptr : (double2 *)(base + cs.offB), g.stream, true, &st->launches,
+                          b_late ? g.copy_ev[1] : nullptr)))
       return r;
     first += n;
     cls++;
@@ -2036,6 +2069,9 @@ int bc_gpu_shutdown(void) {
   if (g.ev0) cudaEventDestroy(g.ev0);
   if (g.ev1) cudaEventDestroy(g.ev1);
   if (g.own_stream) cudaStreamDestroy(g.own_stream);
+  if (g.copy_stream) cudaStreamDestroy(g.copy_stream);
+  for (auto &e : g.copy_ev)
+    if (e) cudaEventDestroy(e);
   g_occ.clear();
   g = Ctx();
   return BC_OK;

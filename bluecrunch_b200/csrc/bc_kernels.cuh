@@ -60,6 +60,7 @@ struct ClassParams {
   int M;
   int L1, S1;      // outer pass: L1-point DFTs with stride S1 = M/L1
   int L2, Lr;      // 3 levels: L2-point DFTs with stride Lr; 2 levels: L2 = 1, Lr = S1
+  int op0, nops_fwd;  // the outer forward pass packs operands [op0, op0 + nops_fwd) (nops_fwd 0: all)
   Tw2 tw4M;        // e^{-2 pi i m/(4M)}
   const double2 *pw_fwd;  // e^{+i pi n1/(2 L1)}
   const double2 *pw_inv;  // e^{-i pi n1/(2 L1)} / M

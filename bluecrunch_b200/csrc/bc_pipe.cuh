@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
   table_to_smem(pwS, p.pw_fwd, L);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   const int tiles = p.S1 / W;
-  const int nops = p.sq ? 1 : 2;
+  const int nops = p.nops_fwd ? p.nops_fwd : (p.sq ? 1 : 2);
   const unsigned per_item = (unsigned)(nops * tiles);
   const unsigned total = (unsigned)p.nitems * per_item;  // far below 2^32
   const FastDiv fd_item(per_item), fd_tile((unsigned)tiles);
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
   };
   auto stage_copy = [&](unsigned u, int st) {
     const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
-    const int op = (int)fd_tile.div((unsigned)rem), tl = rem - op * tiles;
+    const int opr = (int)fd_tile.div((unsigned)rem), tl = rem - opr * tiles, op = p.op0 + opr;
     const ItemDesc &it = p.items[item];
     const uint32_t *X = op ? it.B : it.A;
     // word indices fit an int: operands and transforms stay below 2^29 words
@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     cp_async_wait<1>();
     __syncthreads();
     const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
-    const int op = (int)fd_tile.div((unsigned)rem), tl = rem - op * tiles;
+    const int opr = (int)fd_tile.div((unsigned)rem), tl = rem - opr * tiles, op = p.op0 + opr;
     const ItemDesc &it = p.items[item];
     const unsigned nd = (unsigned)(op ? it.ndB : it.ndA);  // below 2^30
     double2 *gbuf = op ? it.bufB : it.bufA;

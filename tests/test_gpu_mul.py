@@ -170,3 +170,17 @@ def test_batch_spanning_several_staging_chunks(gpu, orc):
         assert orc.modcheck(c, a, b, 4)
     small = items[1]
     assert np.array_equal(outs[1], exact(small[0], small[1], len(small[0]) + len(small[1])))
+
+
+def test_pinned_host_operands_large(gpu, orc):
+    # one large product with both operands and the result in pinned host
+    # memory: B crosses on its own stream while the outer pass packs A
+    import torch
+    n = 1 << 21
+    a, b = limbs(n + 41, n), limbs(n + 43, n - 5)
+    ha = torch.from_numpy(a.view(np.int32)).pin_memory()
+    hb = torch.from_numpy(b.view(np.int32)).pin_memory()
+    hc = torch.zeros(a.size + b.size, dtype=torch.int32).pin_memory()
+    for _ in range(2):
+        gpu.mul(ha, hb, CL=a.size + b.size, out=hc)
+        assert np.array_equal(hc.numpy().view(np.uint32), orc.ntt_mul(a, b, a.size + b.size))
