@@ -328,8 +328,8 @@ def gpu_arm(args):
     import oracle
 
     from bluecrunch_b200.replicas import Replicas, job_throughput
-    reps = Replicas()  # N ranks = N independent replicas; no collective on the data path
-    world, rank, local = reps.world, reps.rank, reps.local
+    ranks = Replicas()  # N ranks = N independent replicas; no collective on the data path
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     torch.cuda.set_device(local)
     bc.init(local)
     stream = torch.cuda.current_stream()
@@ -354,7 +354,7 @@ def gpu_arm(args):
     assert oracle.restated().modcheck(host_c, a, b, 4), "GPU product fails the modular check"
 
     def barrier():
-        reps.barrier()
+        ranks.barrier()
         torch.cuda.synchronize()
 
     for _ in range(W):
@@ -384,7 +384,7 @@ def gpu_arm(args):
     bc.time_kernels(False)
     barrier()
     launches = K * per_product  # kernels of this library launched in the timed pass
-    ms = reps.max(ms)
+    ms = ranks.max(ms)
     value = job_throughput(nbytes, ms, world) / 1e9
 
     # ---- e2e: pinned host buffers through the C ABI, copies in the timed region
@@ -396,7 +396,7 @@ def gpu_arm(args):
     t0 = time.perf_counter()
     for _ in range(max(1, K)):
         bc.mul(ha, hb, CL=CL, out=hc)
-    e2e_ms = reps.max((time.perf_counter() - t0) * 1e3 / max(1, K))
+    e2e_ms = ranks.max((time.perf_counter() - t0) * 1e3 / max(1, K))
     assert np.array_equal(hc.numpy().view(np.uint32), host_c)
     e2e = job_throughput(nbytes, e2e_ms, world) / 1e9
 
@@ -526,7 +526,7 @@ def gpu_arm(args):
             "e": e_runs,
         }
         print(json.dumps(line), flush=True)
-    reps.close()
+    ranks.close()
 
 
 def main():

@@ -325,8 +325,12 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
       s_delta = din;
     }
     __syncthreads();
-    // ---- carries into each run; corrected values to shared memory
+    // ---- carries into each run; corrected values to shared memory, or
+    // (runs of 128 bits, every word of the tile inside the product, C on a
+    // 16-byte boundary) each run's four words straight to C
     unsigned long long *hc = srec;
+    const bool whole = nbits == 128 && (reinterpret_cast<uintptr_t>(it.C) & 15) == 0 &&
+                       4ull * (rt + (unsigned long long)nr) <= it.nwords;
     int d = fn_apply(ex, s_delta);  // delta into run k0
 #pragma unroll
     for (int q = 0; q < CARRY_RPT; q++) {
@@ -334,9 +338,15 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
       if (k < nr) {
         u192_add_delta(h[q], d, nbits);
         d = fn_apply(f[q], d);
-        hc[k] = h[q].w[0];
-        hc[HC_STRIDE + k] = h[q].w[1];
-        hc[2 * HC_STRIDE + k] = h[q].w[2];
+        if (whole) {
+          *reinterpret_cast<uint4 *>(it.C + 4 * (rt + (unsigned long long)k)) =
+              make_uint4((uint32_t)h[q].w[0], (uint32_t)(h[q].w[0] >> 32), (uint32_t)h[q].w[1],
+                         (uint32_t)(h[q].w[1] >> 32));
+        } else {
+          hc[k] = h[q].w[0];
+          hc[HC_STRIDE + k] = h[q].w[1];
+          hc[2 * HC_STRIDE + k] = h[q].w[2];
+        }
         if (k + 1 == nr) {
           // the run after the tile's last one, for a word that straddles it:
           // inside this item only when the item ends inside this tile
@@ -355,10 +365,10 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
         }
       }
     }
-    __syncthreads();
     // ---- words of the tile, one per thread per step (coalesced stores).
     // The tile starts on a word boundary (1024 runs of 8b bits).
-    {
+    if (!whole) {  // uniform over the CTA
+      __syncthreads();
       const unsigned long long w0 = rt * (unsigned long long)nbits / 32;
       const unsigned long long wend =
           min(it.nwords, (rt * (unsigned long long)nbits + (unsigned long long)nr * nbits + 31) / 32);
