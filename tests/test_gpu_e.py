@@ -56,3 +56,10 @@ def test_e_hex_matches_reference_cli():
 def test_e_1e7_matches_published_md5():
     md5, _, _ = _e(10000000)
     assert md5 == MD5["10000000"]
+
+
+def test_e_1e9_matches_published_md5():
+    # e to 10^9 digits end to end (series, division and conversion in device
+    # memory), against the md5 published with the reference
+    md5, _, out = _e(1000000000)
+    assert md5 == MD5["1000000000"], out[-2000:]

@@ -184,3 +184,27 @@ def test_pinned_host_operands_large(gpu, orc):
     for _ in range(2):
         gpu.mul(ha, hb, CL=a.size + b.size, out=hc)
         assert np.array_equal(hc.numpy().view(np.uint32), orc.ntt_mul(a, b, a.size + b.size))
+
+
+@pytest.mark.parametrize("al,bl,sq", [(1 << 26, 1 << 26, False), (1 << 27, 1 << 24, False), (1 << 26, 1 << 26, True)])
+def test_full_size_products_modular(gpu, orc, al, bl, sq):
+    # the sweep's largest sizes (2^26 and 2^27 limbs, transforms of 2^27 and
+    # 2^28 points): too large for an exact reference product in a test, so
+    # size-independent properties instead — the product agrees with A*B
+    # modulo four primes (FP64-free, seeded from the reference's CHECKPRIME),
+    # and its top limbs are zero exactly where AL + BL exceeds the product's
+    # length
+    a = limbs(al + 51, al)
+    b = a if sq else limbs(bl + 53, bl)
+    c, st = gpu.mul(a, None if sq else b, CL=al + bl, square=sq, want_stats=True)
+    assert st["max_round_err"] < 0.25 and st["fft_points"] >= 1 << 27
+    assert orc.modcheck(c, a, b, 4)
+    # one flipped bit of A: the new product passes the same check and
+    # differs from the old one (the check is not blind to the input)
+    if not sq:
+        j = al // 3
+        a2 = a.copy()
+        a2[j] ^= 1  # flip the lowest bit of limb j
+        c2 = gpu.mul(a2, b, CL=al + bl)
+        assert orc.modcheck(c2, a2, b, 4)
+        assert not np.array_equal(c, c2)
