@@ -113,6 +113,22 @@ __host__ __device__ __forceinline__ void u192_or_bits(U192 &h, unsigned long lon
 }
 
 __host__ __device__ __forceinline__ RunRec make_run(const double *c, int b) {
+  if (b == 16) {
+    // 8 x 16 bits fill two words exactly: constant shifts, no selects
+    unsigned long long h0 = 0, h1 = 0;
+    long long acc = 0;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      acc += (long long)c[u];
+      const unsigned long long bits = (unsigned long long)acc & 0xffffull;
+      if (u < 4) h0 |= bits << (16 * u);
+      else h1 |= bits << (16 * (u - 4));
+      acc >>= 16;
+    }
+    RunRec r;
+    r.h0 = h0; r.h1 = h1; r.h2 = 0; r.c = acc;
+    return r;
+  }
   U192 h = {{0, 0, 0}};
   long long acc = 0;
   const unsigned long long mask = (1ull << b) - 1;
