@@ -6,8 +6,12 @@
  *   at p == 0 a two-limb seed from a double built from the top three limbs
  *   (the reference scales by UINT32_MAX, not 2^32; kept, the iteration
  *   corrects it).
- * Each level's two products depend on each other, so they are single GPU
- * products; the large ones are where one-product latency matters.
+ * Each level's two products depend on each other, so they are single
+ * products.  Levels below 2^16 limbs run here (each product one GPU call, or
+ * the host's exact schoolbook below 100 limbs); from 2^16 limbs up, the
+ * levels and the quotient run in device memory (bc_gpu_newton) with the same
+ * semantics for every product, sum and difference, so only the operands and
+ * the result cross the bus.
  */
 #include <stdio.h>
 #include <stdlib.h>
