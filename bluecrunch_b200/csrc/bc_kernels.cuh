@@ -15,7 +15,8 @@
 //                 twiddle e^{-2 pi i s k2/(L2 Lr)}
 //   k2_rows       per row of Lr points: forward DFT of A and B, pointwise
 //                 product (or square), inverse DFT — the spectrum never
-//                 leaves the chip
+//                 leaves the chip (rows of 1024 points: k2_rows_w1024, one
+//                 warp per row, bc_rows_warp.cuh)
 //   k2_mid<L,1>   (3 levels) inverse of k2_mid<L,0>
 //   k2_outer_inv  conjugate twiddle -> inverse L1-point DFT -> un-weight and
 //                 1/M -> round (max |x - round(x)| recorded) -> run records:
