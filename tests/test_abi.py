@@ -76,3 +76,42 @@ def test_pipelined_launch_shapes_consistent():
     # every supported length: TMA boxes deliver exactly the bytes each kernel
     # waits for and tiles cover the rows (checked again before every launch)
     assert bc._lib().bc_gpu_check_shapes() == 0
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the behaviour without a GPU")
+def test_no_gpu_no_fallback():
+    # without an sm_100 device the engine refuses (BC_ERR_NO_DEVICE) and a
+    # product raises; there is no CPU path that would compute it instead
+    import numpy as np
+    with pytest.raises(bc.BcError) as e:
+        bc.init(0)
+    assert e.value.code == -8
+    with pytest.raises(bc.BcError):
+        bc.mul(np.arange(1, 300, dtype=np.uint32), np.arange(1, 300, dtype=np.uint32))
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the behaviour without a GPU")
+def test_host_fft_mul_aborts_without_gpu():
+    # the reference's _fft_mul entry point (include/mul.h) aborts with a
+    # message when the GPU engine is unavailable, as the reference aborts on
+    # the widths it cannot pack; it never computes the product on the CPU
+    import subprocess
+    import sys
+    code = (
+        "import ctypes, numpy as np, bluecrunch_b200 as bc\n"
+        "lib = ctypes.CDLL(bc.HOST_LIB)\n"
+        "a = np.arange(1, 2001, dtype=np.uint32); c = np.zeros(4000, dtype=np.uint32)\n"
+        "p = lambda x: x.ctypes.data_as(ctypes.c_void_p)\n"
+        "lib._fft_mul(p(c), ctypes.c_size_t(4000), p(a), ctypes.c_size_t(2000), p(a), ctypes.c_size_t(2000))\n"
+        "print('computed')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "computed" not in r.stdout
+    assert "GPU" in r.stderr
