@@ -488,13 +488,15 @@ def gpu_arm(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         import oracle as orc
         if orc.have_reference("omp"):
-            ral, rbl, rcl, rdt, thr = time_reference(REF_LOG2, reps=3, kind="omp")
+            # a bounded sample of about 10 s of CPU work (0.4 s per product on 16 threads)
+            nrep = 24
+            ral, rbl, rcl, rdt, thr = time_reference(REF_LOG2, reps=nrep, kind="omp")
             rp = bc.plan(ral, rbl, rcl)
             rb_alg = bc.width_limit(rp["fft_points"])
             cpu = {"value": round(alg_bytes(ral, rbl, rcl, rb_alg, False) / rdt / 1e9, 4), "unit": "GB/s",
                    "cores": thr, "kind": "reference",
-                   "sample": "reference _fft_mul from oracle/_ref (OpenMP tasks, %d threads), 3 multiplies of "
-                             "2^20 x 2^20 limbs (largest size it supports), %.3f s each" % (thr, rdt)}
+                   "sample": "reference _fft_mul from oracle/_ref (OpenMP tasks, %d threads), %d multiplies of "
+                             "2^20 x 2^20 limbs (largest size it supports), %.3f s each" % (thr, nrep, rdt)}
         else:
             sa, sb = operands(16)
             t0 = time.perf_counter()
