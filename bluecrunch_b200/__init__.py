@@ -79,6 +79,7 @@ GPU_SYMBOLS = {
     "bc_gpu_radix_leaves": (ctypes.c_int, [ctypes.c_void_p, _sz, ctypes.c_double]),
     "bc_gpu_radix_tree": (ctypes.c_int, [ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_int, ctypes.c_double, ctypes.c_void_p]),
+    "bc_gpu_selftest_wait": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double)]),
     "bc_gpu_newton": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                      _sz, ctypes.c_void_p]),
     "bc_gpu_radix_tree_pow": (ctypes.c_int, [ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz,

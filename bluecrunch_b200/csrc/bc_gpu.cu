@@ -1840,6 +1840,45 @@ int newton_locked(const bc_bignum *den, const bc_bignum *r0, const size_t *level
   return BC_OK;
 }
 
+// A wait that runs out, on purpose and without a fault: one windowed sum of
+// two tiles whose tile counter starts at 1, so tile 0 is never taken and
+// tile 1's lookback has nothing to wait for.  Its bounded spin gives up,
+// flags the sum and the kernel finishes; the host sees the flag.
+int selftest_wait_locked(double *secs) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  const unsigned long long n = 2ull * ADD_TILE;
+  DevBuf buf;
+  const size_t o_r = align256(n * 4), o_sc = o_r + align256(n * 4), o_st = o_sc + 256;
+  int r;
+  if ((r = buf.alloc(o_st + 256))) return r;
+  char *bp = (char *)buf.p;
+  CK(cudaMemsetAsync(bp, 0, o_st + 256, g.stream));
+  const unsigned one = 1;
+  CK(cudaMemcpyAsync(bp + o_sc, &one, 4, cudaMemcpyHostToDevice, g.stream));  // the counter
+  AddSubParams ap;
+  ap.a = WinOp{(const uint32_t *)bp, 0, (long long)n};
+  ap.b = WinOp{(const uint32_t *)bp, 0, 0};
+  ap.r = (uint32_t *)(bp + o_r);
+  ap.n = n;
+  ap.sub = 0;
+  ap.tiles = 2;
+  ap.counter = (unsigned int *)(bp + o_sc);
+  ap.cout = (unsigned int *)(bp + o_sc + 4);
+  ap.flags = (unsigned int *)(bp + o_sc + 8);
+  ap.status = (uint32_t *)(bp + o_st);
+  CK(cudaEventRecord(g.ev0, g.stream));
+  k_addsub_win<<<1, ADD_NT, 0, g.stream>>>(ap);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(g.ev1, g.stream));
+  unsigned flags = 0;
+  CK(cudaMemcpyAsync(&flags, ap.flags, 4, cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, g.ev0, g.ev1));
+  if (secs) *secs = ms * 1e-3;
+  return (flags & 1u) ? BC_ERR_TIMEOUT : BC_OK;
+}
+
 int e_series_locked(uint32_t a, uint32_t b, uint32_t **hP, size_t *PL, uint32_t **hQ, size_t *QL,
                     bc_batch_stats *st) {
   if (!g.init) return fail(BC_ERR_NOT_INIT);
@@ -2132,6 +2171,11 @@ int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *n
                           uint32_t *out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   return radix_tree_pow_locked(y, ylen, nodes, nnodes, t0, t0len, steps, ntable, alpha, out);
+}
+
+int bc_gpu_selftest_wait(double *seconds) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return selftest_wait_locked(seconds);
 }
 
 int bc_gpu_newton(const bc_bignum *den, const bc_bignum *r0, const size_t *levels, int nlevels, const bc_bignum *num,

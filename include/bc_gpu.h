@@ -184,6 +184,13 @@ typedef struct {
 int bc_gpu_newton(const bc_bignum *den, const bc_bignum *r0, const size_t *levels, int nlevels, const bc_bignum *num,
                   size_t pdiv, bc_bignum_out *out);
 
+/* Diagnostic (no counterpart in the reference): runs one carry lookback
+ * whose predecessor never publishes, so its bounded wait runs out; returns
+ * BC_ERR_TIMEOUT (the wait gave up and flagged the sum) and the kernel's
+ * time in *seconds.  The context stays usable.  Shows that a wait that
+ * cannot end ends the kernel with an error status instead of a hang. */
+int bc_gpu_selftest_wait(double *seconds);
+
 int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nnodes,
                           const uint32_t *t0, size_t t0len, const bc_radix_pow_step *steps, int ntable, double alpha,
                           uint32_t *out);

@@ -208,3 +208,15 @@ def test_full_size_products_modular(gpu, orc, al, bl, sq):
         c2 = gpu.mul(a2, b, CL=al + bl)
         assert orc.modcheck(c2, a2, b, 4)
         assert not np.array_equal(c, c2)
+
+
+def test_bounded_wait_runs_out_without_a_fault(gpu, orc):
+    # a carry lookback whose predecessor never publishes (its tile is never
+    # taken): the bounded spin gives up, flags the sum and the kernel ends;
+    # the host gets BC_ERR_TIMEOUT and the context stays usable
+    import ctypes
+    secs = ctypes.c_double(0.0)
+    rc = gpu._lib().bc_gpu_selftest_wait(ctypes.byref(secs))
+    assert rc == -4, rc  # BC_ERR_TIMEOUT
+    assert 0.0 < secs.value < 60.0, secs.value
+    _check(gpu, orc, limbs(5, 5000), limbs(6, 4000))
