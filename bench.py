@@ -431,7 +431,9 @@ def gpu_arm(args):
 
     # ---- sweep (device-resident, a few steps each)
     sweep = []
-    if not args.no_sweep and rank == 0:
+    # the per-GPU characterisations (sweep, batches, e) run at N = 1 only: with
+    # N ranks the other ranks would wait for them at the closing barrier
+    if not args.no_sweep and rank == 0 and world == 1:
         for lg, ratio, sq in [(14, 1, False), (16, 1, False), (18, 1, False), (20, 1, False), (22, 1, False),
                               (24, 1, False), (26, 1, False), (27, 1, False),
                               (20, 8, False), (24, 8, False), (27, 8, False),
@@ -468,7 +470,7 @@ def gpu_arm(args):
 
     # ---- batched uneven products (8192 per launch sequence) vs per-call launches
     batched = []
-    if not args.no_batched and rank == 0:
+    if not args.no_batched and rank == 0 and world == 1:
         for sib in (False, True):
             try:
                 batched.append(run_batched(bc, torch, stream, n=args.batch_items, sibling=sib))
@@ -477,7 +479,7 @@ def gpu_arm(args):
 
     # ---- e to N digits end to end (CLI), default mode and, smaller, per call
     e_runs = []
-    if rank == 0 and args.e_digits:
+    if rank == 0 and world == 1 and args.e_digits:
         e_runs.append(run_e(args.e_digits))
         if args.e_per_call:
             e_runs.append(run_e(args.e_per_call, ("--per-call",)))
