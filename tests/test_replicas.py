@@ -72,3 +72,22 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert ln["impl"] == "reference"
     if "unavailable" not in ln:
         assert ln["n_gpus"] == 2 and ln["value"] > 0 and ln["cpu_baseline"]["kind"] == "reference"
+
+
+def test_reference_arm_json_contract():
+    # the reference arm's line carries the keys the bench contract names
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [json.loads(ln) for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    ln = lines[0]
+    if "unavailable" in ln:
+        return
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in ln, k
+    assert ln["metric"] == "exact_mul_GBps" and ln["unit"] == "GB/s" and ln["higher_is_better"] is True
+    assert ln["e2e"]["h2d_bytes_per_step"] == 0 and ln["e2e"]["d2h_bytes_per_step"] == 0
+    assert ln["cpu_baseline"]["value"] == ln["value"] and ln["cpu_baseline"]["cores"] >= 1
+    assert "workload" in ln["config"]
