@@ -479,8 +479,10 @@ def gpu_arm(args):
 
     # ---- e to N digits end to end (CLI), default mode and, smaller, per call
     e_runs = []
-    if rank == 0 and world == 1 and args.e_digits:
-        e_runs.append(run_e(args.e_digits))
+    e_list = [int(x) for x in str(args.e_digits).split(",") if x.strip() and int(x) > 0]
+    if rank == 0 and world == 1 and e_list:
+        for nd in e_list:
+            e_runs.append(run_e(nd))
         if args.e_per_call:
             e_runs.append(run_e(args.e_per_call, ("--per-call",)))
             e_runs.append(run_e(args.e_per_call))
@@ -544,7 +546,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-items", type=int, default=8192)
-    ap.add_argument("--e-digits", type=int, default=100000000, help="e to this many digits (0: skip)")
+    ap.add_argument("--e-digits", default="100000000,1000000000",
+                    help="e to these numbers of digits, comma-separated (0: skip)")
     ap.add_argument("--e-per-call", type=int, default=0,
                     help="also e to this many digits with one GPU product per call, and in the default mode")
     args = ap.parse_args()
