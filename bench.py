@@ -46,6 +46,107 @@ def alg_bytes(AL, BL, CL, b, square):
     return 4 * (AL + BL + CL) + (3 - (1 if square else 0)) * 2 * 32 * nc
 
 
+# ---------------------------------------------------------------- formula width
+# The byte formula's b is the width limit of the transform length the engine
+# picks for a product.  The reference arm must not load the engine, so the
+# length choice (shape_for / lengths / make_plan in csrc/bc_gpu.cu) is
+# restated here over the same width table; tests/test_bench_contract.py checks
+# it against bc_gpu_plan for many sizes.
+_ROW_LENS = (128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096)
+_SMALL_LENS = (256, 512, 768, 1024, 1536, 2048, 3072, 4096)
+_OUTER_LENS = (64, 128, 256, 512)
+_ROW_PREF = (1024, 768, 1536, 512, 2048, 3072, 4096)
+_MAX_M = 1 << 30
+
+
+def _pass_tile_w(L):
+    return 1024 // L if 1024 // L >= 8 else 8
+
+
+def _pow2part(x):
+    return x & -x
+
+
+def shape_levels(M):
+    """Levels of the kernel shape for transform length M (0: no shape)."""
+    if M < 256 or M > _MAX_M:
+        return 0
+    p2 = M // 3 if M % 3 == 0 else M
+    if p2 & (p2 - 1):
+        return 0
+    if M <= 4096:
+        return 1 if M in _SMALL_LENS else 0
+    for L1 in _OUTER_LENS:
+        if M % L1 == 0 and (M // L1) in _ROW_LENS and _pow2part(M // L1) >= _pass_tile_w(L1):
+            return 2
+    for Lr in _ROW_PREF:
+        if M % Lr:
+            continue
+        R = M // Lr
+        for L1 in _OUTER_LENS:
+            if R % L1:
+                continue
+            L2 = R // L1
+            if L2 < 64 or L2 > 512 or (L2 & (L2 - 1)) or L2 > L1:
+                continue
+            if _pow2part(Lr) < _pass_tile_w(L2) or _pow2part(L2 * Lr) < _pass_tile_w(L1):
+                continue
+            return 3
+    return 0
+
+
+def _lengths():
+    out = []
+    p = 256
+    while p <= _MAX_M:
+        for m in (p, 3 * p // 2):
+            if m <= _MAX_M and shape_levels(m):
+                out.append(m)
+        p *= 2
+    return sorted(set(out))
+
+
+def _width_table(path=os.path.join(ROOT, "bluecrunch_b200", "tune", "widths.txt")):
+    table = {}
+    if os.path.exists(path):
+        for ln in open(path):
+            f = ln.split()
+            if len(f) >= 2 and not ln.startswith("#") and 8 <= int(f[1]) <= 24:
+                table[int(f[0])] = int(f[1])
+    return table
+
+
+def width_limit_of(M, table=None):
+    table = _width_table() if table is None else table
+    if M in table:
+        return table[M]
+    return max(8, min(24, math.floor(23.0 - 0.3 * math.log2(M))))
+
+
+def formula_plan(AL, BL, CL=None, square=False):
+    """(M, width limit at M) of the product, as the engine plans it."""
+    CL = CL or AL + BL
+    AL, BL = min(AL, CL), min(BL, CL)
+    table = _width_table()
+    nd = lambda x, b: (32 * x + b - 1) // b  # noqa: E731
+    best = None
+    first_fit = 0
+    for M in _lengths():
+        if first_fit and M > 4 * first_fit:
+            break
+        bmax = min(width_limit_of(M, table), 24)
+        if bmax < 8 or nd(AL, bmax) + nd(BL, bmax) > 2 * M + 1:
+            continue
+        first_fit = first_fit or M
+        cost = M * (2 if shape_levels(M) == 3 else 1)
+        if best is not None and cost >= best[0]:
+            continue
+        best = (cost, M)
+    if best is None:
+        raise ValueError("no transform length fits %d x %d limbs" % (AL, BL))
+    return best[1], width_limit_of(best[1], table)
+
+
 def operands(log2n, square=False, ratio=1):
     import oracle
     n = 1 << log2n
@@ -178,7 +279,36 @@ def time_reference(log2n=REF_LOG2, reps=3, kind="omp"):
     return a.size, b.size, CL, dt, ref.threads()
 
 
+def reference_cli_e(digits, threads=None):
+    """e to `digits` digits by the reference's own CLI (main.c:169-219) built
+    from its sources into oracle/_ref/omp (OpenMP tasks in place of Cilk
+    spawns, all host threads unless `threads`), wall time and md5 of e.txt."""
+    import hashlib
+    import tempfile
+    import oracle
+    cli = oracle.reference_cli("omp")
+    if not os.path.exists(cli):
+        return None
+    env = dict(os.environ)
+    nthr = threads or os.cpu_count() or 1
+    env["OMP_NUM_THREADS"] = str(nthr)
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        res = subprocess.run([cli, str(digits)], cwd=d, capture_output=True, text=True, timeout=1800, env=env)
+        wall = time.perf_counter() - t0
+        if res.returncode != 0:
+            return {"digits": digits, "mode": "reference CLI", "error": res.stderr[-300:]}
+        md5 = hashlib.md5(open(os.path.join(d, "e.txt"), "rb").read()).hexdigest()
+    pub = json.load(open(os.path.join(ROOT, "tests", "golden", "e_md5.json")))["published"]["digits_to_md5"]
+    return {"digits": digits, "mode": "reference CLI (oracle/_ref/omp/bluecrunch_ref, %d threads)" % nthr,
+            "wall_s": round(wall, 3), "threads": nthr, "md5": md5, "md5_matches_published": pub.get(str(digits)) == md5}
+
+
 def reference_arm(args):
+    """The reference's own _fft_mul (bigfloat/mul.c:108-174), compiled from its
+    sources into oracle/_ref/omp, timed on all host threads.  Loads nothing of
+    this repository's engine: the byte formula's width comes from
+    formula_plan (the engine's length choice restated over its width table)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -186,7 +316,6 @@ def reference_arm(args):
     if not oracle.have_reference("omp"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build time)"}))
         return
-    import bluecrunch_b200 as bc
     K, W = args.steps, args.warmup
     ref = oracle.reference("omp")
     a, b = operands(REF_LOG2)
@@ -197,8 +326,7 @@ def reference_arm(args):
     for _ in range(K):
         ref.fft_mul(a, b, CL, parallel=True)
     dt = (time.perf_counter() - t0) / K
-    p = bc.plan(a.size, b.size, CL)
-    b_alg = bc.width_limit(p["fft_points"])
+    _, b_alg = formula_plan(a.size, b.size, CL)
     gbs = alg_bytes(a.size, b.size, CL, b_alg, False) / dt / 1e9
     threads = ref.threads()
     print(json.dumps({
@@ -322,6 +450,57 @@ def run_e(digits, extra=()):
             "phases_s": phases, "md5": md5, "md5_matches_published": pub.get(str(digits)) == md5}
 
 
+def same_config_mul(bc, torch, stream, cpu, log2n=REF_LOG2, reps=20):
+    """The reference arm's workload (2^20 x 2^20 limbs) on this engine:
+    device-resident (CUDA events) and end to end through bc_gpu_mul with
+    pinned and with pageable host buffers (copies inside the timed region)."""
+    import oracle
+    a, b = operands(log2n)
+    AL, BL = a.size, b.size
+    CL = AL + BL
+    _, b_alg = formula_plan(AL, BL, CL)
+    nbytes = alg_bytes(AL, BL, CL, b_alg, False)
+    da = torch.from_numpy(a.view(np.int32)).cuda()
+    db = torch.from_numpy(b.view(np.int32)).cuda()
+    dc = torch.zeros(CL, dtype=torch.int32, device="cuda")
+    for _ in range(3):
+        bc.mul(da, db, CL=CL, out=dc)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        bc.mul(da, db, CL=CL, out=dc)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_ms = e0.elapsed_time(e1) / reps
+    want = dc.cpu().numpy().view(np.uint32).copy()
+    ok = oracle.restated().modcheck(want, a, b, 4)
+    res = {"workload": "exact multiply 2^20 x 2^20 limbs (the reference arm's and cpu_baseline's workload)",
+           "unit": "GB/s", "higher_is_better": True, "width_for_formula": b_alg,
+           "gpu_device": {"value": round(nbytes / (dev_ms * 1e-3) / 1e9, 2), "ms_per_step": round(dev_ms, 4)},
+           "modcheck": bool(ok)}
+    ha = torch.from_numpy(a.view(np.int32)).pin_memory()
+    hb = torch.from_numpy(b.view(np.int32)).pin_memory()
+    hc = torch.zeros(CL, dtype=torch.int32).pin_memory()
+    for kind, (xa, xb, xc) in (("pinned", (ha, hb, hc)),
+                               ("pageable", (a, b, np.zeros(CL, dtype=np.uint32)))):
+        bc.mul(xa, xb, CL=CL, out=xc)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            bc.mul(xa, xb, CL=CL, out=xc)
+        e_ms = (time.perf_counter() - t0) * 1e3 / reps
+        got = xc.numpy().view(np.uint32) if hasattr(xc, "numpy") else xc
+        res["gpu_e2e_" + kind] = {"value": round(nbytes / (e_ms * 1e-3) / 1e9, 2), "ms_per_step": round(e_ms, 4),
+                                  "h2d_bytes_per_step": 4 * (AL + BL), "d2h_bytes_per_step": 4 * CL,
+                                  "matches_device_result": bool(np.array_equal(got, want))}
+    res["reference"] = {"value": cpu["value"], "cores": cpu["cores"], "sample": cpu["sample"]}
+    res["gpu_e2e_pageable_over_reference"] = round(res["gpu_e2e_pageable"]["value"] / cpu["value"], 1)
+    res["gpu_device_over_reference"] = round(res["gpu_device"]["value"] / cpu["value"], 1)
+    del da, db, dc
+    return res
+
+
 def gpu_arm(args):
     import torch
     import bluecrunch_b200 as bc
@@ -417,14 +596,20 @@ def gpu_arm(args):
     roof = None
     if dom:
         achieved = per_kernel_bytes.get(dom, 0) / (avg[dom] * 1e-3) / 1e9
-        traffic = None
+        # DRAM bytes per launch are not measurable without a profiler: the
+        # figure comes from the stored ncu capture of this kernel and length
+        traffic, traffic_src = None, None
         tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
         if os.path.exists(tf):
-            tr = json.load(open(tf)).get(dom)
+            tj = json.load(open(tf))
+            tr = tj.get(dom)
             if tr and tr.get("fft_points") == M:
                 traffic = tr.get("dram_bytes_per_launch")
+                traffic_src = "stored ncu capture (profiles/ncu_traffic.json, %s), not measured in this run" % (
+                    tr.get("captured") or tj.get("captured") or "date not recorded")
         roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
+                "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": per_kernel_bytes.get(dom),
                 "kernel_ms": {k: round(v, 4) for k, v in avg.items()},
                 "kernel_share": {k: round(v / sum(avg.values()), 4) for k, v in avg.items()}}
@@ -510,6 +695,26 @@ def gpu_arm(args):
             cpu = {"value": round(alg_bytes(sa.size, sb.size, sa.size + sb.size, bc.width_limit(rp["fft_points"]), False) / dt / 1e9, 4),
                    "unit": "GB/s", "cores": 1, "kind": "port", "sample": "oracle restatement, one 2^16 x 2^16 multiply"}
 
+    # ---- same-workload pairs with the reference, at the sizes it can run:
+    # (1) the exact multiply of 2^20 x 2^20 limbs (the cpu_baseline workload),
+    #     device-resident and through the C ABI with host buffers;
+    # (2) e to 10^7 digits by this repository's CLI and by the reference CLI.
+    same = []
+    if rank == 0 and world == 1 and not args.no_cpu and cpu and cpu.get("kind") == "reference":
+        try:
+            same.append(same_config_mul(bc, torch, stream, cpu))
+        except Exception as exc:
+            same.append({"workload": "exact multiply 2^20 x 2^20 limbs", "error": str(exc)[:300]})
+        if args.e_same:
+            g = run_e(args.e_same)
+            r = reference_cli_e(args.e_same)
+            pair = {"workload": "e to %d decimal digits, end to end (CLI, output files, md5)" % args.e_same,
+                    "unit": "s", "higher_is_better": False, "gpu": g, "reference": r}
+            if r and g.get("wall_s") and r.get("wall_s"):
+                pair["reference_over_gpu"] = round(r["wall_s"] / g["wall_s"], 2)
+                pair["same_digits"] = g.get("md5") == r.get("md5")
+            same.append(pair)
+
     if rank == 0:
         line = {
             "metric": "exact_mul_GBps", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
@@ -530,6 +735,7 @@ def gpu_arm(args):
             "sweep": sweep,
             "batched": batched,
             "e": e_runs,
+            "same_config": same,
         }
         print(json.dumps(line), flush=True)
     ranks.close()
@@ -550,6 +756,8 @@ def main():
                     help="e to these numbers of digits, comma-separated (0: skip)")
     ap.add_argument("--e-per-call", type=int, default=0,
                     help="also e to this many digits with one GPU product per call, and in the default mode")
+    ap.add_argument("--e-same", type=int, default=10000000,
+                    help="e to this many digits by this CLI and by the reference CLI (same workload; 0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

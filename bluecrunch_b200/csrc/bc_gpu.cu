@@ -454,18 +454,25 @@ KInfo get_small(int M, bool sq) {
   return {};
 }
 
-std::map<const void *, int> g_occ;  // resident CTAs per SM, per kernel
+// Grid cap (resident CTAs per SM x SMs) per (device, kernel): the dynamic
+// shared-memory attribute is a per-device setting of the function, so a call
+// on another device (bc_gpu_mul_noalloc takes the caller's current device)
+// sets it there too.
+std::map<std::pair<int, const void *>, int> g_occ;
 
 int prepare(const KInfo &k, int *grid_cap) {
-  auto it = g_occ.find(k.fn);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  auto it = g_occ.find({dev, k.fn});
   if (it == g_occ.end()) {
     if (k.smem > 48 * 1024) CK(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
-    int n = 0;
+    int n = 0, sms = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k.fn, k.threads, k.smem));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (n < 1) n = 1;
-    it = g_occ.emplace(k.fn, n).first;
+    it = g_occ.emplace(std::make_pair(dev, k.fn), n * std::max(sms, 1)).first;
   }
-  *grid_cap = it->second * g.sm_count;
+  *grid_cap = it->second;
   return BC_OK;
 }
 
@@ -2322,12 +2329,13 @@ int bc_gpu_kernel_times(const char **names, double *ms, int cap) {
 
 // ====================================================================== allocation-free entry point
 // bc_gpu_mul_noalloc: the same exact product for callers that cannot
-// allocate device memory themselves or let a library do it — code running
-// inside a captured CUDA stream region, a custom allocator or memory pool
-// that owns the whole device, or an embedding host whose policy forbids
-// cudaMalloc after start-up.  Its scratch (transform buffers, run records,
-// lookback status, descriptor, error slots, twiddle tables) is one
-// file-scope __device__ array; the caller passes device inputs and outputs.
+// allocate device memory themselves or let a library do it — a custom
+// allocator or memory pool that owns the whole device, or an embedding host
+// whose policy forbids cudaMalloc after start-up.  Its scratch (transform
+// buffers, run records, lookback status, descriptor, error slots, twiddle
+// tables) is one file-scope __device__ array; the caller passes device
+// inputs and outputs.  Each call waits for its stream and reads the outcome
+// back, so it cannot be called while that stream is being captured.
 namespace {
 constexpr size_t kNoAllocBytes = size_t(8) << 20;          // 8 MiB of scratch per GPU
 constexpr size_t kNoAllocMaxPoints = size_t(1) << 17;       // transforms up to 2^17 points

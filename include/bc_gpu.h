@@ -221,9 +221,9 @@ int bc_gpu_lengths(size_t *out, int cap);
 int bc_gpu_force_plan(size_t fft_points, int width);
 
 /* Allocation-free product, for callers that cannot allocate device memory
- * or have a library do it (inside a captured stream region, under a pool or
- * allocator that owns the device, in hosts that forbid cudaMalloc after
- * start-up).  No counterpart in the reference.
+ * or have a library do it (under a pool or allocator that owns the device,
+ * in hosts that forbid cudaMalloc after start-up).  No counterpart in the
+ * reference.
  *
  * C, A, B are device pointers of the current device; C must not overlap A or
  * B.  Computes C[0..CL) = A*B mod 2^(32 CL) like bc_gpu_mul, on `stream`
@@ -234,13 +234,12 @@ int bc_gpu_force_plan(size_t fft_points, int width);
  * Scratch is one 8 MiB file-scope __device__ array that every GPU loading
  * this library holds until the process exits; nothing is allocated per call
  * (no cudaMalloc/cudaFree or allocating library routine).  The first call on
- * a device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  Every call on a device shares
- * the array and clears what must start at zero; calls whose GPU work
- * overlaps would race on it.  The function serialises host callers and
- * returns only after its work is complete, so overlap can only come from
- * work enqueued around it (for example replaying a captured graph that
- * contains it on two streams at once). */
+ * a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current.  Every call on a device shares the array and clears
+ * what must start at zero; calls whose GPU work overlaps would race on it.
+ * The function serialises host callers, synchronises `stream` and reads the
+ * outcome back before it returns, so it must not be called on a stream that
+ * is being captured into a CUDA graph. */
 int bc_gpu_mul_noalloc(uint32_t *C, size_t CL, const uint32_t *A, size_t AL,
                        const uint32_t *B, size_t BL, void *stream);
 

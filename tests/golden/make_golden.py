@@ -13,7 +13,10 @@ Sources:
   SplitMix64 operands (oracle.random_limbs), stored as sha256 of the output;
 * e.txt / e-hex.txt md5 from the reference CLI build for 1e3..1e5 digits.
 
-Usage:  python tests/golden/make_golden.py [--ref /root/reference]
+Usage:  python tests/golden/make_golden.py [--ref DIR]
+
+DIR is the reference source tree: $BC_REFERENCE_SRC, else a directory
+named "reference" beside this repository.
 """
 import argparse
 import hashlib
@@ -171,7 +174,7 @@ def e_cli_md5():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("BC_REFERENCE_SRC") or os.path.join(ROOT, "..", "reference"))
     args = ap.parse_args()
     blobs = {
         "known_answers.json": known_answers(args.ref),

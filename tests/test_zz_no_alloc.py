@@ -1,12 +1,13 @@
 """GPU: bc_gpu_mul_noalloc, the allocation-free product for callers that
-cannot allocate device memory (inside captured stream regions, under a pool
-that owns the device, or in hosts that forbid cudaMalloc after start-up).
+cannot allocate device memory (under a pool or allocator that owns the
+device, or in hosts that forbid cudaMalloc after start-up).
 
 Called through the C ABI with device buffers the test allocates itself; the
-result must equal the allocating entry point's (bc_gpu_mul), bit for bit, on
-two calls in a row, and the calls must not change the device's free memory.
-Collected last so a run that stops at the first failure has run every other
-test; passes alone in a fresh process too."""
+result must equal the allocating entry point's (bc_gpu_mul) and the exact
+product (Python integers), bit for bit, on two calls in a row, and the calls
+must not change the device's free memory.  Collected last so a run that
+stops at the first failure has run every other test; passes alone in a fresh
+process too."""
 import ctypes
 
 import numpy as np
@@ -42,7 +43,10 @@ def test_noalloc_matches_bc_gpu_mul_twice():
             torch.cuda.synchronize()
             free_after = torch.cuda.mem_get_info()[0]
             assert rc == 0, bc.BcError(rc)
-            assert np.array_equal(out.cpu().numpy().view(np.uint32), want), (rep, al, bl)
+            got = out.cpu().numpy().view(np.uint32)
+            assert np.array_equal(got, want), (rep, al, bl)
+            exact = bc.from_int(bc.to_int(a) * bc.to_int(b) % (1 << (32 * cl)), cl)
+            assert np.array_equal(got, exact), (rep, al, bl)
             if rep == 1:  # kernels are loaded by now: the call itself allocates nothing
                 assert free_after == free_before
 
