@@ -41,6 +41,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
   }
   return false;
 }
+// After some wait of the CTA gave up: wait once more, longer (about 2^24
+// polls, seconds), for a copy still in flight on `bar` to land, so that no
+// bulk copy writes into the shared memory of a CTA that has exited.  The
+// kernel then stops issuing copies and returns; the item is already flagged.
+constexpr int MBAR_DRAIN_SPINS = 1 << 24;
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, unsigned parity) {
+  for (int i = 0; i < MBAR_DRAIN_SPINS; i++) {
+    if (mbar_try_wait(bar, parity)) return;
+    __nanosleep(256);
+  }
+}
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }

@@ -157,16 +157,25 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
     // e^{-2 pi i col k2/(L2 Lr)} = table index 4 L1 col k2 of the 4M table
     // (global loads issued before the wait so their latency overlaps it)
     twiddle_run(p.tw4M, (uint64_t)4 * p.L1 * col * t, false, (uint64_t)4 * p.L1 * col * TC, w);
-    const bool ok = mbar_wait(&bars[st], (phases >> st) & 1u);
+    const unsigned par = (phases >> st) & 1u;
+    const bool ok = mbar_wait(&bars[st], par);
     phases ^= 1u << st;
-    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
     double2 *bf = buf0 + st * L * W;
 #pragma unroll
     for (int i = 0; i < PTS; i++) {
       v[i] = bf[bidx<L>(t + i * TC, s)];
       if (INV) v[i] = cmulc(v[i], w[i]);
     }
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {
+      // a wait gave up: flag the item, issue nothing more, let the copies in
+      // flight land, leave
+      if (tid == 0) {
+        atomicOr(it.flags, FLAG_TIMEOUT);
+        mbar_drain(&bars[st], par);
+        if (un < total) mbar_drain(&bars[st ^ 1], (phases >> (st ^ 1)) & 1u);
+      }
+      return;
+    }
     block_fft<L, W, INV>(v, t, s, bf, twS);
 #pragma unroll
     for (int i = 0; i < PTS; i++) {
@@ -221,13 +230,20 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_i
     const int col = tile * W + s;
     double2 v[PTS], w[PTS];
     outer_twiddles<TC>(p.tw4M, col, t, w);  // global loads, before the wait
-    const bool ok = mbar_wait(&bars[st], (phases >> st) & 1u);
+    const unsigned par = (phases >> st) & 1u;
+    const bool ok = mbar_wait(&bars[st], par);
     phases ^= 1u << st;
-    if (!ok && tid == 0) atomicOr(it.flags, FLAG_TIMEOUT);
     double2 *bf = buf0 + st * L * W;
 #pragma unroll
     for (int i = 0; i < PTS; i++) v[i] = cmulc(bf[bidx<L>(t + i * TC, s)], w[i]);
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {  // a wait gave up: flag, drain, leave
+      if (tid == 0) {
+        atomicOr(it.flags, FLAG_TIMEOUT);
+        mbar_drain(&bars[st], par);
+        if (un < total) mbar_drain(&bars[st ^ 1], (phases >> (st ^ 1)) & 1u);
+      }
+      return;
+    }
     block_fft<L, W, true>(v, t, s, bf, twS);
     double err = 0.0;
 #pragma unroll
@@ -339,12 +355,14 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
   }
   __syncthreads();
   unsigned u = blockIdx.x;
-  if (tid == 0) {
-    fence_proxy_async_smem();
+  unsigned pend = 0;  // bit k: a copy issued on bars[k] that has not been seen to land
 #pragma unroll
-    for (int q = 0; q < NS; q++) {
-      const unsigned uq = u + q * gridDim.x;
-      if (uq < total) {
+  for (int q = 0; q < NS; q++) {
+    const unsigned uq = u + q * gridDim.x;
+    if (uq < total) {
+      pend |= (1u << q) | (SQ ? 0u : 1u << (2 + q));
+      if (tid == 0) {
+        fence_proxy_async_smem();
         rows_load<L>(bufA0 + q * NR * L, &mA, &bars[q], uq * NR);
         if (!SQ) rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], uq * NR);
       }
@@ -353,6 +371,25 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
   using RS = typename RowSyncOf<L>::type;
   const RS rsync = RowSyncOf<L>::make(rl);  // the threads of this row
   unsigned phases = 0;                      // bit k: parity to wait for on bars[k]
+  bool bad = false;                         // some wait of this thread gave up
+  auto wait_slot = [&](int k) {
+    const bool ok = mbar_wait(&bars[k], (phases >> k) & 1u);
+    if (ok) {
+      phases ^= 1u << k;
+      pend &= ~(1u << k);
+    }
+    bad |= !ok;
+  };
+  // after a wait gave up anywhere in the CTA: flag the item, issue nothing
+  // more, let the copies still in flight land (thread 0 issued them all)
+  auto give_up = [&](const ItemDesc &it) {
+    if (tid == 0) {
+      atomicOr(it.flags, FLAG_TIMEOUT);
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if ((pend >> k) & 1u) mbar_drain(&bars[k], (phases >> k) & 1u);
+    }
+  };
   for (int q = 0; u < total; u += gridDim.x, q = (q + 1 == NS) ? 0 : q + 1) {
     const unsigned un = u + NS * gridDim.x;  // the unit this slot loads next
     const unsigned grow = u * NR + rl;        // this thread's row in the class slab
@@ -362,9 +399,7 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
     double2 *smA = bufA0 + q * NR * L + rl * L;
     double2 *smB = bufA0 + (NS + q) * NR * L + rl * L;
     double2 v[PTS];
-    bool ok = mbar_wait(&bars[q], (phases >> q) & 1u);
-    phases ^= 1u << q;
-    if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+    wait_slot(q);
 #pragma unroll
     for (int i = 0; i < PTS; i++) v[i] = smA[ridx(t + i * TC)];
     rsync();
@@ -376,28 +411,40 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
     } else {
 #pragma unroll
       for (int i = 0; i < PTS; i++) smA[ridx(t + i * TC)] = v[i];  // A's spectrum, read back by this thread only
-      ok = mbar_wait(&bars[2 + q], (phases >> (2 + q)) & 1u);
-      phases ^= 1u << (2 + q);
-      if (!ok && t == 0) atomicOr(it.flags, FLAG_TIMEOUT);
+      wait_slot(2 + q);
 #pragma unroll
       for (int i = 0; i < PTS; i++) v[i] = smB[ridx(t + i * TC)];
       rsync();
       block_fft<L, 1, false, RS, true>(v, t, 0, smB, p.twLr, rsync, twS);
 #pragma unroll
       for (int i = 0; i < PTS; i++) v[i] = cmul(smA[ridx(t + i * TC)], v[i]);
-      __syncthreads();  // every row is done with this B slot and with its spectrum reads
-      if (tid == 0 && un < total) {
-        fence_proxy_async_smem();
-        rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], un * NR);
+      // every row is done with this B slot and with its spectrum reads
+      if (__syncthreads_or(bad)) {
+        give_up(it);
+        return;
+      }
+      if (un < total) {
+        pend |= 1u << (2 + q);
+        if (tid == 0) {
+          fence_proxy_async_smem();
+          rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], un * NR);
+        }
       }
     }
     block_fft<L, 1, true, RS, true>(v, t, 0, smA, p.twLr, rsync, twS);
 #pragma unroll
     for (int i = 0; i < PTS; i++) ra[t + i * TC] = v[i];
-    __syncthreads();  // every row is done with this A slot
-    if (tid == 0 && un < total) {
-      fence_proxy_async_smem();
-      rows_load<L>(bufA0 + q * NR * L, &mA, &bars[q], un * NR);
+    // every row is done with this A slot
+    if (__syncthreads_or(bad)) {
+      give_up(it);
+      return;
+    }
+    if (un < total) {
+      pend |= 1u << q;
+      if (tid == 0) {
+        fence_proxy_async_smem();
+        rows_load<L>(bufA0 + q * NR * L, &mA, &bars[q], un * NR);
+      }
     }
   }
 }

@@ -169,15 +169,20 @@ __global__ void __launch_bounds__(32 * RW_WARPS, 2)
     }
   };
   unsigned ph0 = 0, ph1 = 0;  // parity to wait for on bar0 / bar1
-  // wait for a row's copy (bounded: a wait that gives up flags the row's
-  // item), then move it to registers
-  auto take = [&](double2 (&v)[RW_P], const double2 *src, uint64_t *bar, unsigned &ph, unsigned row) {
-    if (!mbar_wait(bar, ph) && lane == 0) atomicOr(p.items[fd_rows.div(row)].flags, FLAG_TIMEOUT);
+  // wait for a row's copy, then move it to registers.  The wait is bounded;
+  // false when it gave up on any lane of the warp (the loop then stops).
+  auto take = [&](double2 (&v)[RW_P], const double2 *src, uint64_t *bar, unsigned &ph) -> bool {
+    const bool ok = mbar_wait(bar, ph);
+    if (__any_sync(0xffffffffu, !ok)) return false;
     ph ^= 1u;
 #pragma unroll
     for (int i = 0; i < RW_P; i++) v[i] = src[lane + 32 * i];
     __syncwarp();  // the buffer is read: free for the transpose
+    return true;
   };
+  // after a wait gave up: bit 0 / bit 1 = a copy still in flight on bar0 /
+  // bar1, and the row whose item gets flagged
+  unsigned drain = 0, bad_row = 0;
   unsigned r = blockIdx.x * RW_WARPS + wid;
   if (SQ) {
     if (r < total) fetch(buf0, bar0, r, false);
@@ -186,7 +191,11 @@ __global__ void __launch_bounds__(32 * RW_WARPS, 2)
       double2 *const bf = k ? buf1 : buf0;
       uint64_t *const bar = k ? bar1 : bar0;
       double2 va[RW_P];
-      take(va, bf, bar, k ? ph1 : ph0, r);
+      if (!take(va, bf, bar, k ? ph1 : ph0)) {
+        drain = (k ? 2u : 1u) | (r + stride < total ? (k ? 1u : 2u) : 0u);
+        bad_row = r;
+        break;
+      }
       row_dft1024<false>(va, lane, bf, twT);
 #pragma unroll
       for (int i = 0; i < RW_P; i++) va[i] = cmul(va[i], va[i]);
@@ -205,13 +214,21 @@ __global__ void __launch_bounds__(32 * RW_WARPS, 2)
       const bool more = r + stride < total;
       double2 v[RW_P];
       // B: forward transform, spectrum parked in buffer 1 (natural order)
-      take(v, buf1, bar1, ph1, r);
+      if (!take(v, buf1, bar1, ph1)) {
+        drain = 3u;  // A's row r is in flight too
+        bad_row = r;
+        break;
+      }
       row_dft1024<false>(v, lane, buf1, twT);
 #pragma unroll
       for (int i = 0; i < RW_P; i++) buf1[lane + 32 * i] = v[i];
       // A: forward transform, product with B's spectrum (each lane reads
       // back only the entries it wrote)
-      take(v, buf0, bar0, ph0, r);
+      if (!take(v, buf0, bar0, ph0)) {
+        drain = 1u;  // B's next row is not issued yet
+        bad_row = r;
+        break;
+      }
       row_dft1024<false>(v, lane, buf0, twT);
 #pragma unroll
       for (int i = 0; i < RW_P; i++) v[i] = cmul(v[i], buf1[lane + 32 * i]);
@@ -223,6 +240,15 @@ __global__ void __launch_bounds__(32 * RW_WARPS, 2)
 #pragma unroll
       for (int i = 0; i < RW_P; i++) ra[lane + 32 * i] = v[i];
     }
+  }
+  if (drain) {
+    // flag the row's item, let the warp's copies still in flight land, stop
+    if (lane == 0) {
+      atomicOr(p.items[fd_rows.div(bad_row)].flags, FLAG_TIMEOUT);
+      if (drain & 1u) mbar_drain(bar0, ph0);
+      if (drain & 2u) mbar_drain(bar1, ph1);
+    }
+    __syncwarp();
   }
 }
 

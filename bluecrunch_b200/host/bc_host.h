@@ -38,5 +38,9 @@ void bc_host_ensure_gpu(void);
 void bc_host_gpu_batch(bc_gpu_item *items, size_t n);
 /* Product of small operands on the host (schoolbook), CT may alias. */
 void bc_small_mul(uint32_t *CT, size_t CL, const uint32_t *AT, size_t AL, const uint32_t *BT, size_t BL);
+/* The BC_VERIFY check: 0 when C = A*B modulo two 32-bit primes (or when
+ * CL < AL+BL), else the prime that failed. */
+uint64_t bc_host_product_check(const uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B,
+                               size_t BL);
 
 #endif

@@ -113,18 +113,42 @@ static int verify_on(void) {
   return v;
 }
 
-static void verify(const uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B, size_t BL) {
+/* 0 when C = A*B passes the check modulo both primes (or cannot be checked,
+ * CL < AL+BL), else the failing prime. */
+uint64_t bc_host_product_check(const uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B,
+                               size_t BL) {
   static const uint64_t primes[2] = {0x9f063b05u, 4294967291u};
-  if (CL < AL + BL) return;
+  if (CL < AL + BL) return 0;
   for (int k = 0; k < 2; k++) {
     uint64_t p = primes[k];
     uint64_t want = ((uint64_t)residue(A, AL, p) * residue(B, BL, p)) % p;
-    if (want != residue(C, CL, p)) {
-      fprintf(stderr, "bluecrunch: GPU product fails the modular check (AL=%zu BL=%zu CL=%zu prime %llx)\n",
-              AL, BL, CL, (unsigned long long)p);
-      abort();
-    }
+    if (want != residue(C, CL, p)) return p;
   }
+  return 0;
+}
+
+static void verify(const uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B, size_t BL) {
+  const uint64_t p = bc_host_product_check(C, CL, A, AL, B, BL);
+  if (p) {
+    fprintf(stderr, "bluecrunch: GPU product fails the modular check (AL=%zu BL=%zu CL=%zu prime %llx)\n", AL, BL,
+            CL, (unsigned long long)p);
+    abort();
+  }
+}
+
+/* Fault injection on the host, for tests of the check above:
+ * BC_FAULT_FLIP_PRODUCT=k flips one bit of the k-th GPU product's result
+ * (counting _fft_mul calls from 1) after the GPU has returned it and before
+ * the check runs.  Unset: no effect. */
+static void maybe_flip(uint32_t *C, size_t CL) {
+  static long target = -1;
+  static unsigned long calls = 0;
+  if (target < 0) {
+    const char *e = getenv("BC_FAULT_FLIP_PRODUCT");
+    target = e ? atol(e) : 0;
+  }
+  if (target <= 0) return;
+  if (__atomic_add_fetch(&calls, 1, __ATOMIC_RELAXED) == (unsigned long)target && CL) C[CL / 2] ^= 1u;
 }
 
 static void count(size_t products, size_t calls, double secs) {
@@ -145,6 +169,7 @@ int _fft_mul(uint32_t *CT, size_t CL, uint32_t *AT, size_t AL, uint32_t *BT, siz
     fprintf(stderr, "_fft_mul: GPU multiply failed (CL=%zu): %s\n", CL, bc_gpu_strerror(rc));
     abort();
   }
+  maybe_flip(CT, CL);
   if (verify_on() && CT != AT && CT != BT) verify(CT, CL, AT, AL, BT, BL);
   return st.width;
 }
