@@ -669,8 +669,16 @@ def gpu_arm(args):
         for nd in e_list:
             e_runs.append(run_e(nd))
         if args.e_per_call:
-            e_runs.append(run_e(args.e_per_call, ("--per-call",)))
-            e_runs.append(run_e(args.e_per_call))
+            pc = run_e(args.e_per_call, ("--per-call",))
+            pc["mode"] = "one GPU product per call (--per-call)"
+            same = [x for x in e_runs if x.get("digits") == args.e_per_call and "wall_s" in x]
+            if not same:
+                same = [run_e(args.e_per_call)]
+                e_runs.append(same[0])
+            if "wall_s" in pc and "wall_s" in same[0]:
+                pc["per_call_over_tree"] = round(pc["wall_s"] / same[0]["wall_s"], 2)
+                pc["same_md5"] = pc.get("md5") == same[0].get("md5")
+            e_runs.append(pc)
 
     # ---- CPU baseline: the reference multiply on the host cores, bounded sample
     cpu = None
@@ -754,8 +762,9 @@ def main():
     ap.add_argument("--batch-items", type=int, default=8192)
     ap.add_argument("--e-digits", default="100000000,1000000000",
                     help="e to these numbers of digits, comma-separated (0: skip)")
-    ap.add_argument("--e-per-call", type=int, default=0,
-                    help="also e to this many digits with one GPU product per call, and in the default mode")
+    ap.add_argument("--e-per-call", type=int, default=1000000000,
+                    help="also e to this many digits with one GPU product per call (0: skip); the default-mode "
+                         "run of the same size comes from --e-digits")
     ap.add_argument("--e-same", type=int, default=10000000,
                     help="e to this many digits by this CLI and by the reference CLI (same workload; 0: skip)")
     args = ap.parse_args()

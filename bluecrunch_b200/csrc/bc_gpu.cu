@@ -30,6 +30,7 @@
 #include "bc_radix.cuh"
 #include "bc_rows_warp.cuh"
 #include "bc_arith.cuh"
+#include "bc_pass16.cuh"
 
 using namespace bc;
 
@@ -124,6 +125,7 @@ struct Ctx {
   int last_cuda = 0;
   bool time_kernels = false;
   bool rows_warp = true;  // 1024-point rows by k2_rows_w1024 ($BC_ROWS_WARP=0: the block kernel)
+  bool pass16 = true;     // outer passes of L1 <= 256 with 16 points per thread ($BC_PASS16=0: 8 points)
   // second operand's copy of a single product from pinned host memory: on
   // copy_stream, so the outer pass packs the first operand meanwhile
   cudaStream_t copy_stream = nullptr;
@@ -380,6 +382,7 @@ struct KInfo {
   unsigned unit_bytes = 0; // bytes the kernel waits for per staged unit (per operand)
   int parts = 1;          // boxes per column group (or per row)
   bool warp_rows = false; // a row kernel with one warp per row and no tensor maps
+  int pts = PTS;          // points per thread of a column pass (tile width = threads / (L / pts))
 };
 
 template <int L>
@@ -411,7 +414,30 @@ KInfo small_info() {
   return {(const void *)k_small<M, SQ>, M / PTS, TileSmem<M, 1>::elems * sizeof(double2), "small", SIG_P};
 }
 
+template <int L>
+KInfo outer_fwd16_info() {
+  using T = Pass16<L>;
+  KInfo k{(const void *)k3_outer_fwd<L>, T::NT, T::SMEM_FWD, "outer_fwd", SIG_P};
+  k.pts = P16;
+  return k;
+}
+template <int L>
+KInfo outer_inv16_info() {
+  using T = Pass16<L>;
+  KInfo k{(const void *)k3_outer_inv<L>, T::NT, T::SMEM_INV, "outer_inv", SIG_P_MAP, PassTile<L>::BOX_ROWS,
+          PassTile<L>::BYTES, PassTile<L>::HALVES};
+  k.pts = P16;
+  return k;
+}
+
 KInfo get_outer(int L, bool inv) {
+  if (g.pass16) {
+    switch (L) {
+      case 64: return inv ? outer_inv16_info<64>() : outer_fwd16_info<64>();
+      case 128: return inv ? outer_inv16_info<128>() : outer_fwd16_info<128>();
+      case 256: return inv ? outer_inv16_info<256>() : outer_fwd16_info<256>();
+    }
+  }
   switch (L) {
     case 64: return inv ? outer_inv_info<64>() : outer_fwd_info<64>();
     case 128: return inv ? outer_inv_info<128>() : outer_fwd_info<128>();
@@ -554,8 +580,8 @@ bool shape_launch_ok(const Shape &s, bool sq) {
     const KInfo kmf = get_mid(s.L2, false), kmi = get_mid(s.L2, true);
     if (!kmf.fn || !kmi.fn || kmf.smem > kMaxSmemPerCta || kmi.smem > kMaxSmemPerCta) return false;
   }
-  const int W1 = ko.threads / (s.L1 / PTS);
-  if (S1 % W1 || W1 % 8) return false;
+  const int W1 = ko.threads / (s.L1 / ko.pts);
+  if (S1 % W1 || W1 % 8 || ki.threads / (s.L1 / ki.pts) != W1) return false;
   if ((size_t)(W1 / 8) * ki.parts * 128 * ki.box != ki.unit_bytes || (size_t)ki.box * ki.parts != (size_t)s.L1)
     return false;
   const int NR = kr.warp_rows ? 1 : kr.threads / ((int)Lr / PTS);
@@ -565,7 +591,7 @@ bool shape_launch_ok(const Shape &s, bool sq) {
   if (s.levels == 3) {
     KInfo km = get_mid(s.L2, false);
     if (!km.fn) return false;
-    const int W2 = km.threads / (s.L2 / PTS);
+    const int W2 = km.threads / (s.L2 / km.pts);
     if (Lr % W2 || W2 % 8) return false;
     if ((size_t)(W2 / 8) * km.parts * 128 * km.box != km.unit_bytes || (size_t)km.box * km.parts != (size_t)s.L2)
       return false;
@@ -585,7 +611,7 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
   if (s.levels == 1) return launch(get_small(s.M, sq), n, p, nl, stream, timed);
   const cuuint64_t M16 = (cuuint64_t)s.M * 16, S1 = (cuuint64_t)p.S1, Lr = (cuuint64_t)p.Lr;
   KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
-  const int W1 = ko.threads / (s.L1 / PTS);
+  const int W1 = ko.threads / (s.L1 / ko.pts);
   const int nops = sq ? 1 : 2;
   if (b_ready && !sq) {
     // operand A is on the device, B still crossing: pack A, then wait for B
@@ -605,7 +631,7 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
     const cuuint64_t dims[4] = {2 * Lr, (cuuint64_t)s.L2, (cuuint64_t)s.L1, (cuuint64_t)n};
     const cuuint64_t str[3] = {Lr * 16, S1 * 16, M16};
     KInfo km = get_mid(s.L2, false);
-    const int W2 = km.threads / (s.L2 / PTS);
+    const int W2 = km.threads / (s.L2 / km.pts);
     const cuuint32_t box[4] = {16, (cuuint32_t)km.box, 1, 1};
     // the boxes of one tile must deliver exactly what the kernel waits for
     if ((size_t)(W2 / 8) * km.parts * 128 * km.box != km.unit_bytes || (size_t)km.box * km.parts != (size_t)s.L2)
@@ -637,7 +663,7 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
   }
   if (s.levels == 3) {
     KInfo km = get_mid(s.L2, true);
-    const int W2 = km.threads / (s.L2 / PTS);
+    const int W2 = km.threads / (s.L2 / km.pts);
     if ((r = launch(km, n * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, &midA))) return r;
   }
   {
@@ -2092,6 +2118,8 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
   {
     const char *rw = getenv("BC_ROWS_WARP");
     g.rows_warp = !(rw && rw[0] == '0');
+    const char *p16 = getenv("BC_PASS16");
+    g.pass16 = !(p16 && p16[0] == '0');
   }
   load_width_file(c.tune_path);
   g.init = true;
