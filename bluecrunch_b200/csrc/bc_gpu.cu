@@ -31,6 +31,7 @@
 #include "bc_rows_warp.cuh"
 #include "bc_arith.cuh"
 #include "bc_pass16.cuh"
+#include "bc_block.cuh"
 
 using namespace bc;
 
@@ -126,6 +127,7 @@ struct Ctx {
   bool time_kernels = false;
   bool rows_warp = true;  // 1024-point rows by k2_rows_w1024 ($BC_ROWS_WARP=0: the block kernel)
   bool pass16 = true;     // outer passes of L1 <= 256 with 16 points per thread ($BC_PASS16=0: 8 points)
+  bool fused = false;     // three-level middle in one kernel where it applies ($BC_FUSED=1; default: separate passes)
   // second operand's copy of a single product from pinned host memory: on
   // copy_stream, so the outer pass packs the first operand meanwhile
   cudaStream_t copy_stream = nullptr;
@@ -383,6 +385,7 @@ struct KInfo {
   int parts = 1;          // boxes per column group (or per row)
   bool warp_rows = false; // a row kernel with one warp per row and no tensor maps
   int pts = PTS;          // points per thread of a column pass (tile width = threads / (L / pts))
+  bool coop = false;      // cooperative launch: every CTA resident (its warps wait on one another)
 };
 
 template <int L>
@@ -514,7 +517,8 @@ int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunc
   if (mB) b = *mB;
   else b = a;
   void *args[3] = {&pc, &a, &b};
-  CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
+  if (k.coop) CK(cudaLaunchCooperativeKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
+  else CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
   (*nlaunch)++;
   if (timed && g.time_kernels) {
     cudaEvent_t e;
@@ -546,12 +550,12 @@ int get_encoder() {
 
 // FLOAT64 elements, 128-byte swizzle, innermost box dimension 16 doubles.
 int encode_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
-               const cuuint32_t *box) {
+               const cuuint32_t *box, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B) {
   int r = get_encoder();
   if (r) return r;
   cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   CUresult cr = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void *>(base), dims, strides,
-                         box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) {
     if (g.verbose) fprintf(stderr, "bc_gpu: cuTensorMapEncodeTiled failed (%d)\n", (int)cr);
@@ -599,6 +603,19 @@ bool shape_launch_ok(const Shape &s, bool sq) {
   return true;
 }
 
+// The fused middle pass covers three-level shapes with 1024-point rows and
+// L2 = 64 or 128 (on with $BC_FUSED=1).
+bool fused_ok(const Shape &s) {
+  return g.fused && s.levels == 3 && s.Lr == RW_L && (s.L2 == 64 || s.L2 == 128);
+}
+KInfo get_fused(int L2, bool sq) {
+  const void *fn = L2 == 64 ? (sq ? (const void *)k4_mid_fused<64, true> : (const void *)k4_mid_fused<64, false>)
+                            : (sq ? (const void *)k4_mid_fused<128, true> : (const void *)k4_mid_fused<128, false>);
+  KInfo k{fn, 32 * RW_WARPS, BLK_SMEM, "mid_fused", SIG_P_MAP2};
+  k.coop = true;
+  return k;
+}
+
 // The pass sequence of one class (all items share shape and squaring).  The
 // items' A and B buffers are the contiguous slabs slabA / slabB (item i at
 // i*M).  Scratch (records, lookback status, counter) must be set up and the
@@ -626,45 +643,61 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
   } else if ((r = launch(ko, n * nops * (long long)(S1 / W1), p, nl, stream, timed))) {
     return r;
   }
-  CUtensorMap midA, midB;
-  if (s.levels == 3) {
+  if (fused_ok(s) && p.blkdone) {
+    // the middle (column pass, row products, inverse column pass) in one
+    // persistent cooperative kernel; per-block counters in p.blkdone
+    const KInfo kf = get_fused(s.L2, sq);
+    const long long items = (n * s.L1 + BLK_LAG_I) * (long long)s.L2 * (sq ? 3 : 4);
+    // column tiles by TMA: 4-d view (2*Lr doubles, L2 rows, L1 blocks, items),
+    // boxes of 8 complex columns x L2 rows, unswizzled
     const cuuint64_t dims[4] = {2 * Lr, (cuuint64_t)s.L2, (cuuint64_t)s.L1, (cuuint64_t)n};
     const cuuint64_t str[3] = {Lr * 16, S1 * 16, M16};
-    KInfo km = get_mid(s.L2, false);
-    const int W2 = km.threads / (s.L2 / km.pts);
-    const cuuint32_t box[4] = {16, (cuuint32_t)km.box, 1, 1};
-    // the boxes of one tile must deliver exactly what the kernel waits for
-    if ((size_t)(W2 / 8) * km.parts * 128 * km.box != km.unit_bytes || (size_t)km.box * km.parts != (size_t)s.L2)
-      return fail(BC_ERR_INVALID);
-    if ((r = encode_map(&midA, slabA, 4, dims, str, box))) return r;
-    if (!sq && (r = encode_map(&midB, slabB, 4, dims, str, box))) return r;
-    if ((r = launch(km, n * nops * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB)))
-      return r;
-  }
-  if (get_rows(s.Lr, sq).warp_rows) {
-    // one warp per row, plain loads and stores: no tensor maps
-    KInfo kr = get_rows(s.Lr, sq);
-    const long long rows = n * (long long)(s.M / s.Lr);
-    if ((r = launch(kr, (rows + RW_WARPS - 1) / RW_WARPS, p, nl, stream, timed))) return r;
+    const cuuint32_t box[4] = {16, (cuuint32_t)s.L2, 1, 1};
+    CUtensorMap fA, fB;
+    if ((r = encode_map(&fA, slabA, 4, dims, str, box, CU_TENSOR_MAP_SWIZZLE_NONE))) return r;
+    if (!sq && (r = encode_map(&fB, slabB, 4, dims, str, box, CU_TENSOR_MAP_SWIZZLE_NONE))) return r;
+    if ((r = launch(kf, (items + RW_WARPS - 1) / RW_WARPS, p, nl, stream, timed, &fA, sq ? &fA : &fB))) return r;
   } else {
-    KInfo kr = get_rows(s.Lr, sq);
-    const int NR = kr.threads / (s.Lr / PTS);
-    const cuuint64_t rows = (cuuint64_t)n * (cuuint64_t)(s.M / s.Lr);
-    const cuuint64_t dims[3] = {16, Lr / 8, rows};
-    const cuuint64_t str[2] = {128, Lr * 16};
-    const cuuint32_t box[3] = {16, (cuuint32_t)kr.box, (cuuint32_t)NR};
-    if ((size_t)kr.parts * 128 * kr.box * NR != kr.unit_bytes || (size_t)kr.box * kr.parts != (size_t)(Lr / 8) ||
-        (s.M / s.Lr) % NR != 0)
-      return fail(BC_ERR_INVALID);
-    CUtensorMap rA, rB;
-    if ((r = encode_map(&rA, slabA, 3, dims, str, box))) return r;
-    if (!sq && (r = encode_map(&rB, slabB, 3, dims, str, box))) return r;
-    if ((r = launch(kr, (long long)(rows / NR), p, nl, stream, timed, &rA, sq ? &rA : &rB))) return r;
-  }
-  if (s.levels == 3) {
-    KInfo km = get_mid(s.L2, true);
-    const int W2 = km.threads / (s.L2 / km.pts);
-    if ((r = launch(km, n * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, &midA))) return r;
+    CUtensorMap midA, midB;
+    if (s.levels == 3) {
+      const cuuint64_t dims[4] = {2 * Lr, (cuuint64_t)s.L2, (cuuint64_t)s.L1, (cuuint64_t)n};
+      const cuuint64_t str[3] = {Lr * 16, S1 * 16, M16};
+      KInfo km = get_mid(s.L2, false);
+      const int W2 = km.threads / (s.L2 / km.pts);
+      const cuuint32_t box[4] = {16, (cuuint32_t)km.box, 1, 1};
+      // the boxes of one tile must deliver exactly what the kernel waits for
+      if ((size_t)(W2 / 8) * km.parts * 128 * km.box != km.unit_bytes || (size_t)km.box * km.parts != (size_t)s.L2)
+        return fail(BC_ERR_INVALID);
+      if ((r = encode_map(&midA, slabA, 4, dims, str, box))) return r;
+      if (!sq && (r = encode_map(&midB, slabB, 4, dims, str, box))) return r;
+      if ((r = launch(km, n * nops * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB)))
+        return r;
+    }
+    if (get_rows(s.Lr, sq).warp_rows) {
+      // one warp per row, plain loads and stores: no tensor maps
+      KInfo kr = get_rows(s.Lr, sq);
+      const long long rows = n * (long long)(s.M / s.Lr);
+      if ((r = launch(kr, (rows + RW_WARPS - 1) / RW_WARPS, p, nl, stream, timed))) return r;
+    } else {
+      KInfo kr = get_rows(s.Lr, sq);
+      const int NR = kr.threads / (s.Lr / PTS);
+      const cuuint64_t rows = (cuuint64_t)n * (cuuint64_t)(s.M / s.Lr);
+      const cuuint64_t dims[3] = {16, Lr / 8, rows};
+      const cuuint64_t str[2] = {128, Lr * 16};
+      const cuuint32_t box[3] = {16, (cuuint32_t)kr.box, (cuuint32_t)NR};
+      if ((size_t)kr.parts * 128 * kr.box * NR != kr.unit_bytes || (size_t)kr.box * kr.parts != (size_t)(Lr / 8) ||
+          (s.M / s.Lr) % NR != 0)
+        return fail(BC_ERR_INVALID);
+      CUtensorMap rA, rB;
+      if ((r = encode_map(&rA, slabA, 3, dims, str, box))) return r;
+      if (!sq && (r = encode_map(&rB, slabB, 3, dims, str, box))) return r;
+      if ((r = launch(kr, (long long)(rows / NR), p, nl, stream, timed, &rA, sq ? &rA : &rB))) return r;
+    }
+    if (s.levels == 3) {
+      KInfo km = get_mid(s.L2, true);
+      const int W2 = km.threads / (s.L2 / km.pts);
+      if ((r = launch(km, n * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, &midA))) return r;
+    }
   }
   {
     const cuuint64_t dims[3] = {2 * S1, (cuuint64_t)s.L1, (cuuint64_t)n};
@@ -1016,6 +1049,15 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   const size_t off_err = off; off += align256(nw * 8);
   const size_t off_flags = off; off += align256(nw * 4);
   const size_t off_ctr = off; off += 256 * (classes.size() + 1);
+  // per-block counters of the fused middle pass, per class that uses it
+  std::map<std::pair<size_t, bool>, size_t> blk_off;
+  const size_t off_blk = off;
+  for (auto &c : classes) {
+    const Shape &cs = works[c.second[0]]->pl.shape;
+    if (!fused_ok(cs)) continue;
+    blk_off[c.first] = off - off_blk;
+    off += align256((size_t)8 * c.second.size() * cs.L1);
+  }
   const size_t off_status = off; off += align256(status_words * 4);
   const size_t zero_end = off;
   const size_t off_desc = off; off += align256(nw * sizeof(ItemDesc));
@@ -1140,6 +1182,11 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     p.nitems = (int)n;
     p.sq = sq ? 1 : 0;
     p.counter = ctr + 64 * cls;
+    p.blkdone = nullptr;
+    if (blk_off.count(c.first)) p.blkdone = (unsigned int *)(base + off_blk + blk_off[c.first]);
+    p.slabA = (double2 *)(base + slab[c.first].offA);
+    p.slabB = sq ? nullptr : (double2 *)(base + slab[c.first].offB);
+    p.slab_elems = align256(s.M * 16) / 16;
     unsigned long long tiles = 0;
     for (size_t k = first; k < first + n; k++) tiles += works[order[k]]->pl.ntiles;
     p.carry_tiles = tiles;
@@ -2120,6 +2167,8 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
     g.rows_warp = !(rw && rw[0] == '0');
     const char *p16 = getenv("BC_PASS16");
     g.pass16 = !(p16 && p16[0] == '0');
+    const char *fu = getenv("BC_FUSED");
+    g.fused = fu && fu[0] == '1';
   }
   load_width_file(c.tune_path);
   g.init = true;

@@ -71,6 +71,12 @@ struct ClassParams {
   int sq;                 // every item of the class squares (one operand)
   unsigned int *counter;  // k_carry dynamic tile counter (zeroed before launch)
   unsigned long long carry_tiles;  // total k_carry tiles over the class
+  // fused middle pass (three levels): per block (nitems * L1 of them) the
+  // count of finished column items, then of finished row items; zeroed
+  // before launch.  Null: the middle runs as separate passes.
+  unsigned int *blkdone;
+  double2 *slabA, *slabB;          // the class's A and B slabs (item i at slab + i*slab_elems)
+  unsigned long long slab_elems;
 };
 
 // e^{-2 pi i m/(4M)} for m = s*(4k-1) with s < S, k < 4M/(4S): m < 4M when

@@ -81,6 +81,43 @@ def test_block_row_kernel_for_1024_point_rows():
     assert p.returncode == 0 and p.stdout.strip().endswith("OK"), p.stderr[-2000:]
 
 
+_FUSED = r"""
+import sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {tests!r})
+import numpy as np
+import bluecrunch_b200 as bc
+import oracle
+from conftest import limbs
+bc.init(0)
+R = oracle.restated()
+# M = 2^22 (64 x 64 x 1024), 2^23 (128 x 64 x 1024), 2^24 (128 x 128 x 1024)
+for n in (1 << 21, 1 << 22, 1 << 23):
+    a, b = limbs(n + 1, n), limbs(n + 2, n)
+    c, st = bc.mul(a, b, CL=2 * n, want_stats=True)
+    assert bc.plan(n, n)["levels"] == 3
+    ok = np.array_equal(c, R.ntt_mul(a, b, 2 * n)) if n <= (1 << 21) else R.modcheck(c, a, b, 4)
+    assert ok, n
+    s = bc.mul(a, None, CL=2 * n, square=True)
+    assert (np.array_equal(s, R.ntt_mul(a, a, 2 * n)) if n <= (1 << 21) else R.modcheck(s, a, a, 4)), n
+bc.time_kernels(True)
+bc.mul(a, b, CL=2 * n)
+assert "mid_fused" in [k for k, _ in bc.kernel_times()], bc.kernel_times()
+print("OK")
+"""
+
+
+def test_fused_middle_pass():
+    # BC_FUSED=1: the three-level middle (column pass, row products, inverse
+    # column pass) in one persistent cooperative kernel (k4_mid_fused)
+    import subprocess
+    import sys
+    root = os.path.dirname(HERE)
+    env = dict(os.environ, BC_FUSED="1")
+    p = subprocess.run([sys.executable, "-c", _FUSED.format(root=root, tests=HERE)], env=env,
+                       capture_output=True, text=True, timeout=900)
+    assert p.returncode == 0 and p.stdout.strip().endswith("OK"), p.stderr[-2000:]
+
+
 @pytest.mark.parametrize("n", [100, 2048, 30000, 1 << 18, 1 << 20])
 def test_squaring(gpu, orc, n):
     a = limbs(n + 23, n)
