@@ -128,6 +128,7 @@ struct Ctx {
   bool rows_warp = true;  // 1024-point rows by k2_rows_w1024 ($BC_ROWS_WARP=0: the block kernel)
   bool pass16 = true;     // outer passes of L1 <= 256 with 16 points per thread ($BC_PASS16=0: 8 points)
   bool fused = false;     // three-level middle in one kernel where it applies ($BC_FUSED=1; default: separate passes)
+  bool share_b = true;    // one B transform for items with the same device B ($BC_SHARE_B=0: one per item)
   // second operand's copy of a single product from pinned host memory: on
   // copy_stream, so the outer pass packs the first operand meanwhile
   cudaStream_t copy_stream = nullptr;
@@ -205,6 +206,7 @@ struct Plan {
   size_t ndA = 0, ndB = 0;
   size_t nwords = 0, nruns = 0, ntiles = 0;
   bool square = false;
+  size_t CL = 0;
 };
 
 size_t ndigits(size_t XL, int b) { return (32 * (uint64_t)XL + b - 1) / b; }
@@ -213,10 +215,13 @@ size_t ndigits(size_t XL, int b) { return (32 * (uint64_t)XL + b - 1) / b; }
 // 3-level shape adds a read+write of every operand and of the product.
 double shape_cost(const Shape &s) { return (double)s.M * (s.levels == 3 ? 2.0 : 1.0); }
 
+void plan_finish(Plan &pl);
+
 bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl, size_t maxM = 0) {
   pl = Plan();
   pl.AL = std::min(AL, CL);
   pl.BL = std::min(BL, CL);
+  pl.CL = CL;
   pl.square = square;
   bool found = false;
   double best = 0;
@@ -247,15 +252,20 @@ bool make_plan(size_t AL, size_t BL, size_t CL, bool square, int bcap, Plan &pl,
     pl.b = b;
   }
   if (!found) return false;
+  plan_finish(pl);
+  return true;
+}
+
+// The quantities of a plan that follow from its shape and width.
+void plan_finish(Plan &pl) {
   const size_t M = pl.shape.M;
   const int b = pl.b;
   pl.ndA = ndigits(pl.AL, b);
   pl.ndB = ndigits(pl.BL, b);
   const size_t prod_words = (2 * M * (uint64_t)b) / 32;
-  pl.nwords = std::min(CL, prod_words);
+  pl.nwords = std::min(pl.CL, prod_words);
   pl.nruns = std::min((size_t)(2 * M / 8), (pl.nwords * 32 + 8 * b - 1) / (8 * b));
   pl.ntiles = std::max<size_t>(1, (pl.nruns + CARRY_TILE_RUNS - 1) / CARRY_TILE_RUNS);
-  return true;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -629,21 +639,21 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
   const cuuint64_t M16 = (cuuint64_t)s.M * 16, S1 = (cuuint64_t)p.S1, Lr = (cuuint64_t)p.Lr;
   KInfo ko = get_outer(s.L1, false), ki = get_outer(s.L1, true);
   const int W1 = ko.threads / (s.L1 / ko.pts);
-  const int nops = sq ? 1 : 2;
+  // forward operands: every item's A, then the B slab's slots (items sharing
+  // a B share a slot)
+  const long long nb = sq ? 0 : (long long)p.nb;
   if (b_ready && !sq) {
     // operand A is on the device, B still crossing: pack A, then wait for B
     ClassParams pa = p, pb = p;
-    pa.op0 = 0;
-    pa.nops_fwd = 1;
-    pb.op0 = 1;
-    pb.nops_fwd = 1;
+    pa.fwd_ops = 1;
+    pb.fwd_ops = 2;
     if ((r = launch(ko, n * (long long)(S1 / W1), pa, nl, stream, timed))) return r;
     CK(cudaStreamWaitEvent(stream, b_ready, 0));
-    if ((r = launch(ko, n * (long long)(S1 / W1), pb, nl, stream, timed))) return r;
-  } else if ((r = launch(ko, n * nops * (long long)(S1 / W1), p, nl, stream, timed))) {
+    if ((r = launch(ko, nb * (long long)(S1 / W1), pb, nl, stream, timed))) return r;
+  } else if ((r = launch(ko, (n + nb) * (long long)(S1 / W1), p, nl, stream, timed))) {
     return r;
   }
-  if (fused_ok(s) && p.blkdone) {
+  if (fused_ok(s) && p.blkdone && (sq || p.nb == n)) {
     // the middle (column pass, row products, inverse column pass) in one
     // persistent cooperative kernel; per-block counters in p.blkdone
     const KInfo kf = get_fused(s.L2, sq);
@@ -669,8 +679,9 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
       if ((size_t)(W2 / 8) * km.parts * 128 * km.box != km.unit_bytes || (size_t)km.box * km.parts != (size_t)s.L2)
         return fail(BC_ERR_INVALID);
       if ((r = encode_map(&midA, slabA, 4, dims, str, box))) return r;
-      if (!sq && (r = encode_map(&midB, slabB, 4, dims, str, box))) return r;
-      if ((r = launch(km, n * nops * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB)))
+      const cuuint64_t dimsB[4] = {dims[0], dims[1], dims[2], (cuuint64_t)std::max<long long>(nb, 1)};
+      if (!sq && (r = encode_map(&midB, slabB, 4, dimsB, str, box))) return r;
+      if ((r = launch(km, (n + nb) * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB)))
         return r;
     }
     if (get_rows(s.Lr, sq).warp_rows) {
@@ -690,7 +701,9 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
         return fail(BC_ERR_INVALID);
       CUtensorMap rA, rB;
       if ((r = encode_map(&rA, slabA, 3, dims, str, box))) return r;
-      if (!sq && (r = encode_map(&rB, slabB, 3, dims, str, box))) return r;
+      // B's rows by slot: nb slots of M/Lr rows
+      const cuuint64_t dimsB[3] = {16, Lr / 8, (cuuint64_t)std::max<long long>(nb, 1) * (cuuint64_t)(s.M / s.Lr)};
+      if (!sq && (r = encode_map(&rB, slabB, 3, dimsB, str, box))) return r;
       if ((r = launch(kr, (long long)(rows / NR), p, nl, stream, timed, &rA, sq ? &rA : &rB))) return r;
     }
     if (s.levels == 3) {
@@ -743,6 +756,9 @@ int arena_reserve(size_t bytes) {
   cudaError_t e = cudaMalloc(&g.arena, want);
   if (e != cudaSuccess) {
     cudaGetLastError();
+    // give back what the scratch pool keeps (DevBuf), then try the exact size
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, g.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     want = bytes;
     e = cudaMalloc(&g.arena, want);
     if (e != cudaSuccess) {
@@ -1026,13 +1042,54 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   off += align256(stage_in);
   const size_t off_stage_out = off;
   off += align256(stage_out);
+  // ---- shared B transforms: in a class of two or more levels, items whose B
+  // is the same device array (same pointer and length) get one B slot, packed
+  // and transformed once (the splitting tree's P_l*Q_r and Q_l*Q_r share Q_r,
+  // the nodes of a conversion depth share their power); they take the widest
+  // of their widths, which fits each of them at the class's length
+  std::vector<int> bslot(nw, -1);
+  std::map<std::pair<size_t, bool>, std::vector<int>> owners;  // per class: item (class order) of each slot
+  for (auto &c : classes) {
+    std::vector<int> &own = owners[c.first];
+    if (c.first.second) continue;
+    std::map<std::pair<const uint32_t *, size_t>, std::vector<size_t>> groups;
+    for (size_t k = 0; k < c.second.size(); k++) {
+      const size_t i = c.second[k];
+      const Plan &pl = works[i]->pl;
+      const bc_mul_desc &d = items[works[i]->idx];
+      if (pl.shape.levels >= 2 && !hostB[i] && !g.forced_width && g.share_b) groups[{d.B, pl.BL}].push_back(k);
+      else { bslot[i] = (int)own.size(); own.push_back((int)k); }
+    }
+    for (auto &gr : groups) {
+      int bmax = 0;
+      for (size_t k : gr.second) bmax = std::max(bmax, works[c.second[k]]->pl.b);
+      int slot = -1;
+      for (size_t k : gr.second) {
+        Work *w = works[c.second[k]];
+        if (w->bcap < bmax) {  // redone at a narrower width: keeps its own B
+          bslot[c.second[k]] = (int)own.size();
+          own.push_back((int)k);
+          continue;
+        }
+        if (slot < 0) {
+          slot = (int)own.size();
+          own.push_back((int)k);
+        }
+        if (w->pl.b != bmax) {
+          w->pl.b = bmax;
+          plan_finish(w->pl);
+        }
+        bslot[c.second[k]] = slot;
+      }
+    }
+  }
   struct ClassSlab { size_t offA = 0, offB = 0; };
   std::map<std::pair<size_t, bool>, ClassSlab> slab;
   for (auto &c : classes) {
     const size_t M = c.first.first, n = c.second.size();
     ClassSlab cs;
     cs.offA = off; off += n * align256(M * 16);
-    if (!c.first.second) { cs.offB = off; off += n * align256(M * 16); }
+    if (!c.first.second) { cs.offB = off; off += owners[c.first].size() * align256(M * 16); }
     slab[c.first] = cs;
   }
   size_t status_words = 0;
@@ -1061,6 +1118,14 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   const size_t off_status = off; off += align256(status_words * 4);
   const size_t zero_end = off;
   const size_t off_desc = off; off += align256(nw * sizeof(ItemDesc));
+  // B-slot owners of every class, after the descriptors (copied with them)
+  std::map<std::pair<size_t, bool>, size_t> own_off;
+  size_t own_words = 0;
+  for (auto &c : classes) {
+    own_off[c.first] = own_words;
+    own_words += owners[c.first].size();
+  }
+  off += align256(own_words * 4);
   int r = arena_reserve(off);
   if (r) return r;
   char *base = g.arena;
@@ -1137,7 +1202,8 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
       it.AL = pl.AL; it.BL = pl.BL; it.CL = d.CL;
       it.ndA = pl.ndA; it.ndB = pl.square ? pl.ndA : pl.ndB;
       it.bufA = (double2 *)(base + cs.offA + k * align256(M * 16));
-      it.bufB = pl.square ? nullptr : (double2 *)(base + cs.offB + k * align256(M * 16));
+      it.bslot = pl.square ? 0 : bslot[i];
+      it.bufB = pl.square ? nullptr : (double2 *)(base + cs.offB + (size_t)it.bslot * align256(M * 16));
       it.rec = nullptr; it.status = nullptr;
       if (pl.shape.levels > 1) {
         it.rec = (RunRec *)(base + slots[i].off_rec);
@@ -1159,10 +1225,20 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   ItemDesc *ddesc = (ItemDesc *)(base + off_desc);
   // descriptors and, later, the outcomes go through one pinned block: the
   // descriptors at its start, the outcomes (err, flags) after them
-  const size_t pin_desc = align256(nw * sizeof(ItemDesc)), pin_outc = off_flags + nw * 4 - off_err;
+  // (the B-slot owners right after the descriptors, as in the arena)
+  const size_t desc_bytes = align256(nw * sizeof(ItemDesc)) + own_words * 4;
+  const size_t pin_desc = align256(desc_bytes), pin_outc = off_flags + nw * 4 - off_err;
   if ((r = pin_small_reserve(pin_desc + pin_outc))) return r;
   memcpy(g.pin_small, desc.data(), nw * sizeof(ItemDesc));
-  CK(cudaMemcpyAsync(ddesc, g.pin_small, nw * sizeof(ItemDesc), cudaMemcpyHostToDevice, g.stream));
+  {
+    int *po = (int *)((char *)g.pin_small + align256(nw * sizeof(ItemDesc)));
+    for (auto &c : classes) {
+      const std::vector<int> &own = owners[c.first];
+      std::copy(own.begin(), own.end(), po + own_off[c.first]);
+    }
+  }
+  CK(cudaMemcpyAsync(ddesc, g.pin_small, desc_bytes, cudaMemcpyHostToDevice, g.stream));
+  const int *down = (const int *)((const char *)ddesc + align256(nw * sizeof(ItemDesc)));
   unsigned int *ctr = (unsigned int *)(base + off_ctr);
 
   // ---- launches
@@ -1186,6 +1262,9 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     if (blk_off.count(c.first)) p.blkdone = (unsigned int *)(base + off_blk + blk_off[c.first]);
     p.slabA = (double2 *)(base + slab[c.first].offA);
     p.slabB = sq ? nullptr : (double2 *)(base + slab[c.first].offB);
+    p.nb = sq ? 0 : (int)owners[c.first].size();
+    p.bowner = sq ? nullptr : down + own_off[c.first];
+    p.fwd_ops = 0;
     p.slab_elems = align256(s.M * 16) / 16;
     unsigned long long tiles = 0;
     for (size_t k = first; k < first + n; k++) tiles += works[order[k]]->pl.ntiles;
@@ -1353,11 +1432,16 @@ struct DevNum {
   size_t len = 0;
 };
 
-struct DevBuf {  // cudaMalloc'd, freed on scope exit
+// Scratch of the tree and Newton drivers, freed on scope exit.  Stream-ordered
+// (cudaMallocAsync / cudaFreeAsync on the library stream, from the device's
+// default pool, which bc_gpu_init tells to keep freed memory): no device-wide
+// synchronisation per free and no driver allocation per level or operand.
+// Every user of a DevBuf works on the library stream.
+struct DevBuf {
   void *p = nullptr;
-  ~DevBuf() { if (p) cudaFree(p); }
+  ~DevBuf() { if (p) cudaFreeAsync(p, g.stream); }
   int alloc(size_t bytes) {
-    CK(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+    CK(cudaMallocAsync(&p, std::max<size_t>(bytes, 256), g.stream));
     if (poison_on()) CK(cudaMemsetAsync(p, 0xA5, std::max<size_t>(bytes, 256), g.stream));
     return BC_OK;
   }
@@ -2151,6 +2235,14 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
   g.sm_count = prop.multiProcessorCount;
   CK(cudaStreamCreateWithFlags(&g.own_stream, cudaStreamNonBlocking));
   g.stream = g.own_stream;
+  {
+    // the default pool backs the drivers' scratch (DevBuf): keep what they
+    // free for the next level instead of returning it at every synchronisation
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, c.device));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   CK(cudaEventCreate(&g.ev0));
   CK(cudaEventCreate(&g.ev1));
   size_t fre = 0, tot = 0;
@@ -2169,6 +2261,8 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
     g.pass16 = !(p16 && p16[0] == '0');
     const char *fu = getenv("BC_FUSED");
     g.fused = fu && fu[0] == '1';
+    const char *sb = getenv("BC_SHARE_B");
+    g.share_b = !(sb && sb[0] == '0');
   }
   load_width_file(c.tune_path);
   g.init = true;
@@ -2513,6 +2607,7 @@ extern "C" int bc_gpu_mul_noalloc(uint32_t *C, size_t CL, const uint32_t *A, siz
     p.sq = square ? 1 : 0;
     p.counter = ctr;
     p.carry_tiles = pl.ntiles;
+    p.nb = square ? 0 : 1;  // one B slot, its own (bowner null)
     size_t nl = 0;
     int r = launch_class(s, square, p, 1, pl.ntiles, it.bufA, it.bufB, stream, false, &nl);
     if (r) return r;

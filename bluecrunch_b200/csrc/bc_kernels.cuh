@@ -55,13 +55,21 @@ struct ItemDesc {
   int b;
   int square;
   int a16, b16;                   // operand A / B starts on a 16-byte boundary
+  int bslot;                      // slot of B's transform in the class's B slab (shared by items with the same B)
 };
 
 struct ClassParams {
   int M;
   int L1, S1;      // outer pass: L1-point DFTs with stride S1 = M/L1
   int L2, Lr;      // 3 levels: L2-point DFTs with stride Lr; 2 levels: L2 = 1, Lr = S1
-  int op0, nops_fwd;  // the outer forward pass packs operands [op0, op0 + nops_fwd) (nops_fwd 0: all)
+  // Forward-pass units: the A transform of every item, then the B slab's
+  // slots (nb of them; slot j is B of item bowner[j], null: item j).  Items
+  // with the same B share one slot, so their B is packed and transformed
+  // once.  fwd_ops restricts the outer forward pass to A (1) or B (2)
+  // units; 0 covers both.
+  int fwd_ops;
+  int nb;
+  const int *bowner;
   Tw2 tw4M;        // e^{-2 pi i m/(4M)}
   const double2 *pw_fwd;  // e^{+i pi n1/(2 L1)}
   const double2 *pw_inv;  // e^{-i pi n1/(2 L1)} / M
@@ -78,6 +86,40 @@ struct ClassParams {
   double2 *slabA, *slabB;          // the class's A and B slabs (item i at slab + i*slab_elems)
   unsigned long long slab_elems;
 };
+
+// One unit of a forward pass: operand `op` of item `item` (for B, the owner
+// of slot `slot`), and the unit's index `rest` inside that operand's
+// per_op units.  Units [0, nA) are A's (item-major), the rest B's
+// (slot-major).
+struct FwdUnit {
+  int item, op, slot;
+  unsigned rest;
+};
+__device__ __forceinline__ FwdUnit fwd_unit(const ClassParams &p, unsigned u, unsigned nA, const FastDiv &fd_op,
+                                            unsigned per_op) {
+  FwdUnit f;
+  if (u < nA) {
+    const unsigned i = fd_op.div(u);
+    f.item = (int)i;
+    f.slot = (int)i;
+    f.op = 0;
+    f.rest = u - i * per_op;
+  } else {
+    const unsigned v = u - nA, j = fd_op.div(v);
+    f.slot = (int)j;
+    f.item = p.bowner ? p.bowner[j] : (int)j;
+    f.op = 1;
+    f.rest = v - j * per_op;
+  }
+  return f;
+}
+// A and B unit counts of a forward pass with per_op units per operand.
+__device__ __forceinline__ unsigned fwd_units_a(const ClassParams &p, unsigned per_op) {
+  return p.fwd_ops != 2 ? (unsigned)p.nitems * per_op : 0u;
+}
+__device__ __forceinline__ unsigned fwd_units_b(const ClassParams &p, unsigned per_op) {
+  return (!p.sq && p.fwd_ops != 1) ? (unsigned)p.nb * per_op : 0u;
+}
 
 // e^{-2 pi i m/(4M)} for m = s*(4k-1) with s < S, k < 4M/(4S): m < 4M when
 // k >= 1; for k = 0 it is the conjugate of m = s.

@@ -161,19 +161,18 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB) k3_outer_fwd(C
   table_to_smem(pwS, p.pw_fwd, L);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   const int tiles = p.S1 / W;
-  const int nops = p.nops_fwd ? p.nops_fwd : (p.sq ? 1 : 2);
-  const unsigned per_item = (unsigned)(nops * tiles);
-  const unsigned total = (unsigned)p.nitems * per_item;  // far below 2^32
-  const FastDiv fd_item(per_item), fd_tile((unsigned)tiles);
+  const unsigned nA = fwd_units_a(p, (unsigned)tiles);
+  const unsigned total = nA + fwd_units_b(p, (unsigned)tiles);  // far below 2^32
+  const FastDiv fd_tile((unsigned)tiles);
   // limb staging: as k2_outer_fwd (every row segment of a tile shares one
   // alignment below a 16-byte boundary)
   auto seg_shift = [&](int tl, int b, bool al16) -> int {
     return al16 ? (int)((((long long)tl * W * b >> 5) - 1) & 3) : 0;
   };
   auto stage_copy = [&](unsigned u) {
-    const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
-    const int opr = (int)fd_tile.div((unsigned)rem), tl = rem - opr * tiles, op = p.op0 + opr;
-    const ItemDesc &it = p.items[item];
+    const FwdUnit f = fwd_unit(p, u, nA, fd_tile, (unsigned)tiles);
+    const int tl = (int)f.rest, op = f.op;
+    const ItemDesc &it = p.items[f.item];
     const uint32_t *X = op ? it.B : it.A;
     const int XL = (int)(op ? it.BL : it.AL);
     const int b = it.b;
@@ -207,9 +206,9 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB) k3_outer_fwd(C
   if (u < total) stage_copy(u);
   cp_async_commit();
   for (; u < total; u += gridDim.x) {
-    const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
-    const int opr = (int)fd_tile.div((unsigned)rem), tl = rem - opr * tiles, op = p.op0 + opr;
-    const ItemDesc &it = p.items[item];
+    const FwdUnit f = fwd_unit(p, u, nA, fd_tile, (unsigned)tiles);
+    const int tl = (int)f.rest, op = f.op;
+    const ItemDesc &it = p.items[f.item];
     const int col = tl * W + s;
     // twiddle table loads first: their latency overlaps the digits and the transform
     const OuterRaw16 twr = outer_raw16<R>(p.tw4M, col, t);

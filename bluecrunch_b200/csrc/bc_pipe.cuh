@@ -117,23 +117,25 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   // unit counts stay far below 2^32 (a class holds at most 2^33 points, 2048 per unit)
   const unsigned tiles = p.Lr / W;
-  const unsigned nops = (INV || p.sq) ? 1 : 2;
-  const unsigned per_op = (unsigned)p.L1 * tiles, per_item = nops * per_op;
-  const unsigned total = (unsigned)p.nitems * per_item;
-  const FastDiv fd_item(per_item), fd_op(per_op), fd_tile(tiles);
-  auto decode = [&](unsigned u, int &item, int &op, int &blk, int &tile) {
-    item = (int)fd_item.div(u);
-    unsigned r = u - (unsigned)item * per_item;
-    op = (int)fd_op.div(r);
-    r -= (unsigned)op * per_op;
-    blk = (int)fd_tile.div(r);
-    tile = (int)(r - (unsigned)blk * tiles);
+  // forward: the A units of every item, then the B slab's slots (map mB's
+  // last coordinate is the slot); inverse: A only
+  const unsigned per_op = (unsigned)p.L1 * tiles;
+  const unsigned nA = INV ? (unsigned)p.nitems * per_op : fwd_units_a(p, per_op);
+  const unsigned total = nA + (INV ? 0u : fwd_units_b(p, per_op));
+  const FastDiv fd_op(per_op), fd_tile(tiles);
+  auto decode = [&](unsigned u, int &item, int &op, int &slot, int &blk, int &tile) {
+    const FwdUnit f = fwd_unit(p, u, nA, fd_op, per_op);
+    item = f.item;
+    op = f.op;
+    slot = f.slot;
+    blk = (int)fd_tile.div(f.rest);
+    tile = (int)(f.rest - (unsigned)blk * tiles);
   };
   auto issue = [&](unsigned u, int st) {
-    int item, op, blk, tile;
-    decode(u, item, op, blk, tile);
+    int item, op, slot, blk, tile;
+    decode(u, item, op, slot, blk, tile);
     fence_proxy_async_smem();
-    tile_load_4d<L, W>(buf0 + st * L * W, op ? &mB : &mA, &bars[st], tile * W, blk, item);
+    tile_load_4d<L, W>(buf0 + st * L * W, op ? &mB : &mA, &bars[st], tile * W, blk, slot);
   };
   if (tid == 0) {
     mbar_init(&bars[0], 1);
@@ -148,8 +150,8 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
   for (; u < total; u += gridDim.x) {
     const unsigned un = u + gridDim.x;
     if (tid == 0 && un < total) issue(un, st ^ 1);
-    int item, op, blk, tile;
-    decode(u, item, op, blk, tile);
+    int item, op, slot, blk, tile;
+    decode(u, item, op, slot, blk, tile);
     const ItemDesc &it = p.items[item];
     double2 *g = (op ? it.bufB : it.bufA) + (unsigned)blk * (unsigned)p.S1;
     const int col = tile * W + s;
@@ -348,6 +350,11 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
   const unsigned rows_item = p.M / L;
   const unsigned total = (unsigned)p.nitems * rows_item / NR;  // far below 2^32
   const FastDiv fd_rows(rows_item);
+  // row of the B slab for class row `row` (item i's B transform sits in its slot)
+  auto brow = [&](unsigned row) -> unsigned {
+    const unsigned item = fd_rows.div(row);
+    return (unsigned)p.items[item].bslot * rows_item + (row - item * rows_item);
+  };
   if (tid == 0) {
 #pragma unroll
     for (int k = 0; k < 4; k++) mbar_init(&bars[k], 1);
@@ -364,7 +371,7 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
       if (tid == 0) {
         fence_proxy_async_smem();
         rows_load<L>(bufA0 + q * NR * L, &mA, &bars[q], uq * NR);
-        if (!SQ) rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], uq * NR);
+        if (!SQ) rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], brow(uq * NR));
       }
     }
   }
@@ -427,7 +434,7 @@ __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
         pend |= 1u << (2 + q);
         if (tid == 0) {
           fence_proxy_async_smem();
-          rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], un * NR);
+          rows_load<L>(bufA0 + (NS + q) * NR * L, &mB, &bars[2 + q], brow(un * NR));
         }
       }
     }
@@ -483,10 +490,9 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
   table_to_smem(pwS, p.pw_fwd, L);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   const int tiles = p.S1 / W;
-  const int nops = p.nops_fwd ? p.nops_fwd : (p.sq ? 1 : 2);
-  const unsigned per_item = (unsigned)(nops * tiles);
-  const unsigned total = (unsigned)p.nitems * per_item;  // far below 2^32
-  const FastDiv fd_item(per_item), fd_tile((unsigned)tiles);
+  const unsigned nA = fwd_units_a(p, (unsigned)tiles);
+  const unsigned total = nA + fwd_units_b(p, (unsigned)tiles);  // far below 2^32
+  const FastDiv fd_tile((unsigned)tiles);
   // Row segment (n1, part) of tile tl starts one word below the word of digit
   // j0 = n1*S1 + tl*W + part*M.  S1 and M are multiples of 128, so that word is
   // n1*(S1 b/32) + part*(M b/32) + (tl*W*b >> 5), with the first two terms
@@ -497,9 +503,9 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     return al16 ? (int)((((long long)tl * W * b >> 5) - 1) & 3) : 0;
   };
   auto stage_copy = [&](unsigned u, int st) {
-    const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
-    const int opr = (int)fd_tile.div((unsigned)rem), tl = rem - opr * tiles, op = p.op0 + opr;
-    const ItemDesc &it = p.items[item];
+    const FwdUnit f = fwd_unit(p, u, nA, fd_tile, (unsigned)tiles);
+    const int tl = (int)f.rest, op = f.op;
+    const ItemDesc &it = p.items[f.item];
     const uint32_t *X = op ? it.B : it.A;
     // word indices fit an int: operands and transforms stay below 2^29 words
     const int XL = (int)(op ? it.BL : it.AL);
@@ -542,9 +548,9 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_f
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    const int item = (int)fd_item.div(u), rem = (int)(u - (unsigned)item * per_item);
-    const int opr = (int)fd_tile.div((unsigned)rem), tl = rem - opr * tiles, op = p.op0 + opr;
-    const ItemDesc &it = p.items[item];
+    const FwdUnit f = fwd_unit(p, u, nA, fd_tile, (unsigned)tiles);
+    const int tl = (int)f.rest, op = f.op;
+    const ItemDesc &it = p.items[f.item];
     const unsigned nd = (unsigned)(op ? it.ndB : it.ndA);  // below 2^30
     double2 *gbuf = op ? it.bufB : it.bufA;
     const int b = it.b;

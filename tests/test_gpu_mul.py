@@ -118,6 +118,49 @@ def test_fused_middle_pass():
     assert p.returncode == 0 and p.stdout.strip().endswith("OK"), p.stderr[-2000:]
 
 
+@pytest.mark.parametrize("bl,als", [(3000, [2900, 3000, 3100, 1000]),            # one length, two levels
+                                    (300000, [290000, 310000, 300000]),         # two levels
+                                    (2 << 20, [(2 << 20) - 5000, 2 << 20, (2 << 20) + 7])])  # three levels
+def test_shared_b_transform(gpu, orc, bl, als):
+    # items of a batch whose B is the same device array share one B slot
+    # (packed and transformed once, at the widest of their widths); every
+    # product must stay exact, also beside items with their own B and squares
+    torch = pytest.importorskip("torch")
+    import numpy as np
+    b = limbs(bl + 5, bl)
+    db = torch.from_numpy(b.view(np.int32)).cuda()
+    items, outs, want = [], [], []
+    for k, al in enumerate(als):
+        a = limbs(al + 11 * k, al)
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        dc = torch.zeros(al + bl, dtype=torch.int32, device="cuda")
+        items.append((da, db, dc))
+        want.append((a, b))
+    other = limbs(bl + 77, bl)
+    do = torch.from_numpy(other.view(np.int32)).cuda()
+    dco = torch.zeros(2 * bl, dtype=torch.int32, device="cuda")
+    dsq = torch.zeros(2 * bl, dtype=torch.int32, device="cuda")
+    descs = (gpu.MulDesc * (len(items) + 2))()
+    for i, (da, dbb, dc) in enumerate(items):
+        descs[i] = gpu.MulDesc(dc.data_ptr(), dc.numel(), da.data_ptr(), da.numel(), dbb.data_ptr(), dbb.numel())
+    descs[len(items)] = gpu.MulDesc(dco.data_ptr(), 2 * bl, do.data_ptr(), bl, db.data_ptr(), bl)
+    descs[len(items) + 1] = gpu.MulDesc(dsq.data_ptr(), 2 * bl, db.data_ptr(), bl, db.data_ptr(), bl)
+    gpu.mul_batch_desc(descs, len(items) + 2)
+    torch.cuda.synchronize()
+    for (a, bb), (_, _, dc) in zip(want, items):
+        got = dc.cpu().numpy().view(np.uint32)
+        if a.size + bb.size <= 1 << 20:
+            assert np.array_equal(got, exact(a, bb, a.size + bb.size)), (a.size, bb.size)
+        else:
+            assert orc.modcheck(got, a, bb, 4), (a.size, bb.size)
+    got_o = dco.cpu().numpy().view(np.uint32)
+    got_s = dsq.cpu().numpy().view(np.uint32)
+    if 2 * bl <= 1 << 20:
+        assert np.array_equal(got_o, exact(other, b, 2 * bl)) and np.array_equal(got_s, exact(b, b, 2 * bl))
+    else:
+        assert orc.modcheck(got_o, other, b, 4) and orc.modcheck(got_s, b, b, 4)
+
+
 @pytest.mark.parametrize("n", [100, 2048, 30000, 1 << 18, 1 << 20])
 def test_squaring(gpu, orc, n):
     a = limbs(n + 23, n)
