@@ -436,18 +436,48 @@ def run_e(digits, extra=()):
         with open(os.path.join(d, "e.txt"), "rb") as f:
             for blk in iter(lambda: f.read(1 << 24), b""):
                 h.update(blk)
-    phases = {}
-    for ln in res.stdout.splitlines():
-        ln = ln.strip()
-        for name in ("Summing", "Dividing", "Writing hex digits", "Converting to decimal", "Writing decimal digits"):
-            if ln.startswith(name) and "[" in ln:
-                try:
-                    phases[name] = float(ln.rsplit("[", 1)[1].split()[0])
-                except ValueError:
-                    pass
+    phases = parse_phases(res.stdout)
     md5 = h.hexdigest()
-    return {"digits": digits, "mode": " ".join(extra) or "tree in device memory", "wall_s": round(wall, 3),
-            "phases_s": phases, "md5": md5, "md5_matches_published": pub.get(str(digits)) == md5}
+    out = {"digits": digits, "mode": " ".join(extra) or "tree in device memory", "wall_s": round(wall, 3),
+           "phases_s": phases, "md5": md5, "md5_matches_published": pub.get(str(digits)) == md5}
+    if "Starting GPU engine" in phases:
+        # process start and GPU context creation vary by a few seconds between
+        # fresh processes; the rest is the computation and the output files
+        out["wall_after_engine_start_s"] = round(wall - phases["Starting GPU engine"], 3)
+    return out
+
+
+PHASES = ("Starting GPU engine", "Summing", "Dividing", "Converting to decimal", "Writing hex digits",
+          "Writing decimal digits")
+
+
+def parse_phases(text):
+    """Phase times of the CLI's output (timers.c format): "<name>... done [s
+    seconds]" on one line, or "<name>..." then inner phases and an indented
+    "Done [s seconds]" at the phase's own indentation."""
+    phases, open_at = {}, {}
+    for raw in text.splitlines():
+        ind = len(raw) - len(raw.lstrip(" "))
+        ln = raw.strip()
+        for name in PHASES:
+            if ln.startswith(name + "..."):
+                if "[" in ln:
+                    try:
+                        phases[name] = float(ln.rsplit("[", 1)[1].split()[0])
+                    except ValueError:
+                        pass
+                else:
+                    open_at[ind] = name
+        # "Done [..]" closes the phase opened at its indentation; a bare
+        # "done [..]" (the phase's line was broken by diagnostic output) the
+        # latest one
+        key = ind if ln.startswith("Done [") else (max(open_at) if open_at and ln.startswith("done [") else None)
+        if key is not None and key in open_at:
+            try:
+                phases[open_at.pop(key)] = float(ln.split("[", 1)[1].split()[0])
+            except ValueError:
+                pass
+    return phases
 
 
 def same_config_mul(bc, torch, stream, cpu, log2n=REF_LOG2, reps=20):

@@ -277,6 +277,12 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
     fprintf(stderr, "Limit Exceeded");
     return -1;
   }
+  /* the GPU engine first, in a phase of its own: opening the device (driver
+   * and context start) takes from under one to several seconds on a fresh
+   * process, and would otherwise land in the first phase that multiplies */
+  task_start(1, "Starting GPU engine");
+  bc_host_ensure_gpu();
+  task_end(1);
   task_start(1, "Summing");
   bigfloat_t P, Q;
   bigfloat_new(P);
