@@ -96,6 +96,9 @@ GPU_SYMBOLS = {
     "bc_gpu_lengths": (ctypes.c_int, [ctypes.POINTER(_sz), ctypes.c_int]),
     "bc_gpu_check_shapes": (ctypes.c_int, []),
     "bc_gpu_load_width_table": (ctypes.c_int, [ctypes.c_char_p]),
+    "bc_gpu_shape_candidates": (ctypes.c_int, [_sz, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "bc_gpu_set_shape": (ctypes.c_int, [_sz, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "bc_gpu_load_shape_table": (ctypes.c_int, [ctypes.c_char_p]),
     "bc_gpu_mul_noalloc": (ctypes.c_int, [ctypes.c_void_p, _sz, ctypes.c_void_p, _sz, ctypes.c_void_p, _sz,
                                           ctypes.c_void_p]),
     "bc_gpu_sync": (ctypes.c_int, []),
@@ -236,6 +239,22 @@ def force_width(width):
 
 def force_plan(fft_points, width):
     _check(_lib().bc_gpu_force_plan(fft_points, width))
+
+
+def shape_candidates(M):
+    """Valid decompositions of transform length M: list of (levels, L1, L2, Lr)."""
+    n = _lib().bc_gpu_shape_candidates(M, None, 0)
+    buf = (ctypes.c_int * (4 * max(n, 1)))()
+    _lib().bc_gpu_shape_candidates(M, buf, n)
+    return [tuple(buf[4 * i:4 * i + 4]) for i in range(n)]
+
+
+def set_shape(M, L1=0, L2=0, Lr=0):
+    """Run transform length M as L1 x L2 x Lr (L2 = 1: two levels); zeros: built-in."""
+    _check(_lib().bc_gpu_set_shape(M, L1, L2, Lr), "bc_gpu_set_shape")
+
+
+SHAPE_FILE = os.path.join(PKG, "tune", "shapes.txt")
 
 
 def lengths():

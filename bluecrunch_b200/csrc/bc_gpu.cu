@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -53,7 +54,9 @@ bool is_row_len(size_t L) {
 }
 size_t pow2part(size_t x) { return x & (~x + 1); }
 
-bool shape_for(size_t M, Shape &s) {
+// The built-in decomposition of transform length M (shape_for below may
+// replace it by a tuned one with the same number of levels).
+bool shape_default(size_t M, Shape &s) {
   if (M < 256 || M > kMaxM) return false;
   const size_t p2 = (M % 3 == 0) ? M / 3 : M;
   if (p2 & (p2 - 1)) return false;
@@ -93,8 +96,8 @@ const std::vector<size_t> &lengths() {
     std::vector<size_t> r;
     for (size_t p = 256; p <= kMaxM; p *= 2) {
       Shape s;
-      if (shape_for(p, s)) r.push_back(p);
-      if (3 * p / 2 <= kMaxM && shape_for(3 * p / 2, s)) r.push_back(3 * p / 2);
+      if (shape_default(p, s)) r.push_back(p);
+      if (3 * p / 2 <= kMaxM && shape_default(3 * p / 2, s)) r.push_back(3 * p / 2);
     }
     std::sort(r.begin(), r.end());
     return r;
@@ -115,9 +118,10 @@ struct Ctx {
   cudaStream_t own_stream = nullptr, stream = nullptr;
   char *arena = nullptr;
   size_t arena_cap = 0, arena_limit = 0;
-  std::map<size_t, Tables> tables;
+  std::map<std::tuple<size_t, int, int, int>, Tables> tables;  // per (M, L1, L2, Lr)
   std::map<size_t, int> width_override;
   std::map<size_t, int> width_file;
+  std::map<size_t, Shape> shape_table;  // tuned decompositions (shapes file, bc_gpu_set_shape)
   int forced_width = 0;
   size_t forced_M = 0;
   double max_err = 0.25;
@@ -146,6 +150,49 @@ struct Ctx {
 
 Ctx g;
 std::recursive_mutex g_mu;
+
+// The decomposition a product of length M runs with: the tuned one when the
+// shapes table has M, else the built-in one.
+bool shape_for(size_t M, Shape &s) {
+  auto it = g.shape_table.find(M);
+  if (it != g.shape_table.end()) {
+    s = it->second;
+    return true;
+  }
+  return shape_default(M, s);
+}
+
+// Structural candidates for length M with as many levels as the built-in
+// shape: two levels L1 x Lr, three levels L1 x L2 x Lr, over the compiled
+// outer, middle and row lengths (launch consistency is checked separately,
+// shape_launch_ok).
+std::vector<Shape> shape_candidates(size_t M) {
+  std::vector<Shape> out;
+  Shape d;
+  if (!shape_default(M, d) || d.levels < 2) return out;
+  for (int L1 : kOuterLens) {
+    if (M % L1) continue;
+    const size_t R = M / L1;
+    if (d.levels == 2) {
+      if (is_row_len(R) && pow2part(R) >= (size_t)pass_tile_w(L1)) {
+        Shape s;
+        s.M = (int)M; s.L1 = L1; s.L2 = 1; s.Lr = (int)R; s.levels = 2;
+        out.push_back(s);
+      }
+      continue;
+    }
+    for (int Lr : kRowLens) {
+      if (R % Lr) continue;
+      const size_t L2 = R / Lr;
+      if (L2 < 64 || L2 > 512 || (L2 & (L2 - 1))) continue;
+      if (pow2part(Lr) < (size_t)pass_tile_w((int)L2) || pow2part(L2 * Lr) < (size_t)pass_tile_w(L1)) continue;
+      Shape s;
+      s.M = (int)M; s.L1 = L1; s.L2 = (int)L2; s.Lr = Lr; s.levels = 3;
+      out.push_back(s);
+    }
+  }
+  return out;
+}
 
 int fail(int code) {
   g.last_error = code;
@@ -361,8 +408,11 @@ Tables tables_at(const TableLayout &t, double2 *dev) {
   return r;
 }
 
+// Tables are cached per decomposition (their layout and entries depend on
+// L1, L2 and Lr, not on M alone).
 int ensure_tables(const Shape &s, Tables **out) {
-  auto it = g.tables.find((size_t)s.M);
+  const auto key = std::make_tuple((size_t)s.M, s.L1, s.L2, s.Lr);
+  auto it = g.tables.find(key);
   if (it != g.tables.end()) { *out = &it->second; return BC_OK; }
   const TableLayout lay = table_layout(s);
   std::vector<double2> host(lay.total);
@@ -375,7 +425,7 @@ int ensure_tables(const Shape &s, Tables **out) {
   // stream, so the first kernels of a new length could read stale tables.
   CK(cudaMemcpyAsync(dev, host.data(), lay.total * sizeof(double2), cudaMemcpyHostToDevice, g.stream));
   CK(cudaStreamSynchronize(g.stream));
-  auto res = g.tables.emplace((size_t)s.M, tables_at(lay, dev));
+  auto res = g.tables.emplace(key, tables_at(lay, dev));
   *out = &res.first->second;
   return BC_OK;
 }
@@ -2265,6 +2315,24 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
     g.share_b = !(sb && sb[0] == '0');
   }
   load_width_file(c.tune_path);
+  {
+    // tuned decompositions: $BC_SHAPE_FILE, else shapes.txt beside the width table
+    const char *sp = getenv("BC_SHAPE_FILE");
+    std::string path = sp ? sp : "";
+    const char *tp = c.tune_path ? c.tune_path : getenv("BC_TUNE_FILE");
+    if (path.empty() && tp && *tp) {
+      path = tp;
+      const size_t slash = path.rfind('/');
+      path = (slash == std::string::npos ? std::string() : path.substr(0, slash + 1)) + "shapes.txt";
+    }
+    if (!path.empty()) {
+      FILE *f = fopen(path.c_str(), "r");
+      if (f) {
+        fclose(f);
+        bc_gpu_load_shape_table(path.c_str());
+      }
+    }
+  }
   g.init = true;
   return BC_OK;
 }
@@ -2441,6 +2509,52 @@ int bc_gpu_lengths(size_t *out, int cap) {
   return (int)v.size();
 }
 
+int bc_gpu_shape_candidates(size_t fft_points, int *out, int cap) {
+  int n = 0;
+  for (const Shape &s : shape_candidates(fft_points)) {
+    if (!shape_launch_ok(s, false) || !shape_launch_ok(s, true)) continue;
+    if (out && n < cap) {
+      out[4 * n] = s.levels;
+      out[4 * n + 1] = s.L1;
+      out[4 * n + 2] = s.L2;
+      out[4 * n + 3] = s.Lr;
+    }
+    n++;
+  }
+  return n;
+}
+
+int bc_gpu_set_shape(size_t fft_points, int L1, int L2, int Lr) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (L1 == 0 && L2 == 0 && Lr == 0) {
+    g.shape_table.erase(fft_points);
+    return BC_OK;
+  }
+  for (const Shape &s : shape_candidates(fft_points))
+    if (s.L1 == L1 && s.L2 == L2 && s.Lr == Lr && shape_launch_ok(s, false) && shape_launch_ok(s, true)) {
+      g.shape_table[fft_points] = s;
+      return BC_OK;
+    }
+  return BC_ERR_INVALID;
+}
+
+int bc_gpu_load_shape_table(const char *path) {
+  if (!path) return BC_ERR_INVALID;
+  FILE *f = fopen(path, "r");
+  if (!f) return BC_ERR_INVALID;
+  char line[256];
+  int bad = 0;
+  while (fgets(line, sizeof line, f)) {
+    if (line[0] == '#') continue;
+    unsigned long long M = 0;
+    int L1 = 0, L2 = 0, Lr = 0;
+    if (sscanf(line, "%llu %d %d %d", &M, &L1, &L2, &Lr) == 4 && bc_gpu_set_shape((size_t)M, L1, L2, Lr) != BC_OK)
+      bad++;
+  }
+  fclose(f);
+  return bad ? BC_ERR_INVALID : BC_OK;
+}
+
 int bc_gpu_force_plan(size_t fft_points, int width) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   if (width != 0 && (width < 8 || width > 24)) return BC_ERR_INVALID;
@@ -2524,7 +2638,8 @@ constexpr int kNoAllocMaxDevices = 64;
 
 struct NoAllocDevice {
   unsigned char *base;  // device address of the scratch array on this device
-  size_t table_M;       // transform length whose tables are in the scratch
+  size_t table_M;       // transform length and split whose tables are in the scratch
+  int table_L1, table_L2, table_Lr;
   int ready;
 };
 NoAllocDevice g_noalloc[kNoAllocMaxDevices];
@@ -2569,11 +2684,14 @@ extern "C" int bc_gpu_mul_noalloc(uint32_t *C, size_t CL, const uint32_t *A, siz
     const TableLayout lay = table_layout(s);
     if (lay.total * sizeof(double2) > kNoAllocTableBytes || pl.ntiles * 4 > kNoAllocStatusBytes)
       return fail(BC_ERR_TOO_LARGE);
-    if (nd.table_M != (size_t)s.M) {
+    if (nd.table_M != (size_t)s.M || nd.table_L1 != s.L1 || nd.table_L2 != s.L2 || nd.table_Lr != s.Lr) {
       CK(cudaStreamSynchronize(stream));  // the staging array and the old tables are no longer in use
       fill_tables(s, lay, g_noalloc_tables);
       CK(cudaMemcpyAsync(nd.base, g_noalloc_tables, lay.total * sizeof(double2), cudaMemcpyHostToDevice, stream));
       nd.table_M = s.M;
+      nd.table_L1 = s.L1;
+      nd.table_L2 = s.L2;
+      nd.table_Lr = s.Lr;
     }
     unsigned char *w = nd.base + kNoAllocWorkOff;
     const size_t M = s.M;

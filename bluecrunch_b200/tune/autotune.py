@@ -9,6 +9,15 @@ which bc_gpu_init loads (bluecrunch_b200.init passes it; C callers set
 BC_TUNE_FILE or bc_gpu_config.tune_path).
 
   python -m bluecrunch_b200.tune.autotune [--max-log2 29] [--target 0.125]
+
+With --shapes it tunes the decomposition instead: for every length of two or
+more levels, each valid split (bc_gpu_shape_candidates: L1 x Lr or
+L1 x L2 x Lr over the compiled pass lengths) runs a full-size product of
+seeded random operands on the GPU (CUDA events, modular check of the
+result), and the fastest goes to tune/shapes.txt, which bc_gpu_init loads
+from beside the width table.
+
+  python -m bluecrunch_b200.tune.autotune --shapes [--max-log2 28]
 """
 import argparse
 import datetime
@@ -44,15 +53,99 @@ def measure(bc, torch, M, b, seed=1):
     return st["max_round_err"]
 
 
+def time_shape(bc, torch, M, shape, reps):
+    """Device time (ms) of one full-size product at length M with the given
+    decomposition, and whether the result passes the modular check."""
+    _, L1, L2, Lr = shape
+    bc.set_shape(M, L1, L2, Lr)
+    b = bc.width_limit(M)
+    n = max(1, (M * b) // 32)
+    a = random_limbs(M + 11, n)
+    c = random_limbs(M + 13, n)
+    bc.force_plan(M, b)
+    try:
+        da = torch.from_numpy(a.view(np.int32)).cuda()
+        db = torch.from_numpy(c.view(np.int32)).cuda()
+        out = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+        _, st = bc.mul(da, db, CL=2 * n, out=out, want_stats=True)  # warm (tables, arena)
+        assert st["fft_points"] == M
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            bc.mul(da, db, CL=2 * n, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        ok = True
+        try:
+            import oracle
+            ok = oracle.restated().modcheck(out.cpu().numpy().view(np.uint32), a, c, 2)
+        except (ImportError, OSError):
+            pass
+        return ms, ok
+    finally:
+        bc.force_plan(0, 0)
+        bc.set_shape(M)
+
+
+def tune_shapes(bc, torch, args):
+    """Per transform length of two or more levels, time every decomposition
+    (bc_gpu_shape_candidates) on a full-size product and keep the fastest."""
+    lines = []
+    for M in bc.lengths():
+        if M > (1 << args.max_log2):
+            break
+        cands = bc.shape_candidates(M)
+        if len(cands) < 2:
+            continue
+        reps = 8 if M <= (1 << 22) else 3
+        res = []
+        for sh in cands:
+            try:
+                ms, ok = time_shape(bc, torch, M, sh, reps)
+            except bc.BcError as exc:  # a split whose product is refused or wrong is not a candidate
+                print("M=%d %s failed: %s" % (M, sh, exc), flush=True)
+                ms, ok = float("inf"), False
+            if not ok:
+                print("M=%d %s: wrong product" % (M, sh), flush=True)
+            res.append((ms if ok else float("inf"), sh))
+        res.sort()
+        best = res[0][1]
+        desc = ", ".join("%dx%dx%d %.4f" % (s[1], s[2], s[3], t) for t, s in res)
+        lines.append((M, best, desc))
+        print("M=%-10d best %s   (%s)" % (M, best, desc), flush=True)
+        torch.cuda.empty_cache()
+    with open(args.out, "w") as fh:
+        fh.write("# transform_points L1 L2 Lr  (bluecrunch_b200/tune/autotune.py --shapes, %s, %s);\n"
+                 "# each line's comment lists every decomposition timed (ms per full-size product)\n"
+                 % (torch.cuda.get_device_name(0), datetime.date.today().isoformat()))
+        for M, (_, L1, L2, Lr), desc in lines:
+            fh.write("%d %d %d %d  # %s\n" % (M, L1, L2, Lr, desc))
+    print("wrote", args.out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--max-log2", type=int, default=29)
     ap.add_argument("--target", type=float, default=0.125)
-    ap.add_argument("--out", default=os.path.join(HERE, "widths.txt"))
+    ap.add_argument("--shapes", action="store_true",
+                    help="tune the decomposition of every length instead of the widths")
+    ap.add_argument("--out", default=None)
     args = ap.parse_args()
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
     import torch
     import bluecrunch_b200 as bc
+
+    if args.shapes:
+        args.out = args.out or os.path.join(HERE, "shapes.txt")
+        bc.init(0)  # the tuned widths; the shapes under test are set one by one
+        for M in bc.lengths():
+            bc.set_shape(M)  # start from the built-in decompositions
+        tune_shapes(bc, torch, args)
+        return
+    args.out = args.out or os.path.join(HERE, "widths.txt")
 
     bc.init(0, tune_path="")  # start from the built-in defaults
     lines = []

@@ -220,6 +220,24 @@ int bc_gpu_lengths(size_t *out, int cap);
 /* Force transform length and width (0, 0 = automatic); for the autotuner. */
 int bc_gpu_force_plan(size_t fft_points, int width);
 
+/* Decompositions of one transform length (no counterpart in the reference,
+ * whose CPU transform has a single recursive form, fft/fft.c:43-96).  A
+ * length of two or more levels can run as several L1 x Lr or L1 x L2 x Lr
+ * splits over the compiled pass lengths; the shape autotuner
+ * (bluecrunch_b200/tune/autotune.py --shapes) times them on the GPU and
+ * writes the fastest per length to tune/shapes.txt, which bc_gpu_init loads
+ * from beside the width table (or $BC_SHAPE_FILE).  No GPU needed for these
+ * calls.
+ *   bc_gpu_shape_candidates: the valid splits of fft_points as
+ *     (levels, L1, L2, Lr) quadruples in out[4*i..4*i+3] (up to cap of them);
+ *     returns how many there are;
+ *   bc_gpu_set_shape: run fft_points with that split (0, 0, 0 = built-in);
+ *     BC_ERR_INVALID if it is not one of the candidates;
+ *   bc_gpu_load_shape_table: lines "M L1 L2 Lr" (L2 = 1 for two levels). */
+int bc_gpu_shape_candidates(size_t fft_points, int *out, int cap);
+int bc_gpu_set_shape(size_t fft_points, int L1, int L2, int Lr);
+int bc_gpu_load_shape_table(const char *path);
+
 /* Allocation-free product, for callers that cannot allocate device memory
  * or have a library do it (under a pool or allocator that owns the device,
  * in hosts that forbid cudaMalloc after start-up).  No counterpart in the

@@ -115,3 +115,30 @@ def test_host_fft_mul_aborts_without_gpu():
     r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=120)
     assert r.returncode != 0 and "computed" not in r.stdout
     assert "GPU" in r.stderr
+
+
+def test_shape_candidates_and_table():
+    # every length of two or more levels offers its built-in split among the
+    # candidates; a candidate can be set and reset, anything else is refused
+    lib = bc._lib()
+    for M in (1 << 13, 3 << 14, 1 << 20, 1 << 22, 1 << 25, 3 << 25, 1 << 28):
+        p = bc.plan(M // 2, M // 2, M)
+        if p["fft_points"] != M:
+            continue
+        cands = bc.shape_candidates(M)
+        assert (p["levels"], p["L1"], p["L2"], p["Lr"]) in cands, (M, p, cands)
+        for lv, L1, L2, Lr in cands:
+            assert lv == p["levels"] and L1 * L2 * Lr == M
+        lv, L1, L2, Lr = cands[-1]
+        bc.set_shape(M, L1, L2, Lr)
+        q = bc.plan(M // 2, M // 2, M)
+        assert (q["L1"], q["L2"], q["Lr"]) == (L1, L2, Lr)
+        assert lib.bc_gpu_check_shapes() == 0
+        bc.set_shape(M)
+        assert lib.bc_gpu_set_shape(M, 3, 5, 7) == -1
+    # the committed table holds candidates only
+    if os.path.exists(bc.SHAPE_FILE):
+        assert lib.bc_gpu_load_shape_table(bc.SHAPE_FILE.encode()) == 0
+        assert lib.bc_gpu_check_shapes() == 0
+        for M in bc.lengths():
+            bc.set_shape(M)
