@@ -52,10 +52,10 @@ def alg_bytes(AL, BL, CL, b, square):
 # length choice (shape_for / lengths / make_plan in csrc/bc_gpu.cu) is
 # restated here over the same width table; tests/test_bench_contract.py checks
 # it against bc_gpu_plan for many sizes.
-_ROW_LENS = (128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096)
-_SMALL_LENS = (256, 512, 768, 1024, 1536, 2048, 3072, 4096)
+_ROW_LENS = (128, 192, 256, 320, 384, 512, 640, 768, 1024, 1280, 1536, 2048, 2560, 3072, 4096)
+_SMALL_LENS = (256, 512, 768, 1024, 1280, 1536, 2048, 2560, 3072, 4096, 5120)
 _OUTER_LENS = (64, 128, 256, 512)
-_ROW_PREF = (1024, 768, 1536, 512, 2048, 3072, 4096)
+_ROW_PREF = (1024, 768, 1536, 512, 2048, 3072, 4096, 1280, 640, 2560)
 _MAX_M = 1 << 30
 
 
@@ -71,10 +71,10 @@ def shape_levels(M):
     """Levels of the kernel shape for transform length M (0: no shape)."""
     if M < 256 or M > _MAX_M:
         return 0
-    p2 = M // 3 if M % 3 == 0 else M
+    p2 = M // 3 if M % 3 == 0 else (M // 5 if M % 5 == 0 else M)
     if p2 & (p2 - 1):
         return 0
-    if M <= 4096:
+    if M <= 5120:
         return 1 if M in _SMALL_LENS else 0
     for L1 in _OUTER_LENS:
         if M % L1 == 0 and (M // L1) in _ROW_LENS and _pow2part(M // L1) >= _pass_tile_w(L1):
@@ -99,7 +99,7 @@ def _lengths():
     out = []
     p = 256
     while p <= _MAX_M:
-        for m in (p, 3 * p // 2):
+        for m in (p, 3 * p // 2, 5 * p // 4):
             if m <= _MAX_M and shape_levels(m):
                 out.append(m)
         p *= 2
@@ -118,9 +118,13 @@ def _width_table(path=os.path.join(ROOT, "bluecrunch_b200", "tune", "widths.txt"
 
 def width_limit_of(M, table=None):
     table = _width_table() if table is None else table
+    default = max(8, min(24, math.floor(23.0 - 0.3 * math.log2(M))))
     if M in table:
         return table[M]
-    return max(8, min(24, math.floor(23.0 - 0.3 * math.log2(M))))
+    longer = [k for k in table if k > M]
+    if longer:  # the width of the next longer tuned length
+        return min(table[min(longer)], default + 4)
+    return default
 
 
 def formula_plan(AL, BL, CL=None, square=False):

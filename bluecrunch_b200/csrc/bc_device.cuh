@@ -82,12 +82,38 @@ __device__ __forceinline__ void dft3(double2 &a, double2 &b, double2 &c) {
   c = csub(m, r);
 }
 
+// 5-point DFT: with s1 = x1+x4, d1 = x1-x4, s2 = x2+x3, d2 = x2-x3 and
+// c_k = cos(2 pi k/5), s_k = sin(2 pi k/5):
+//   X0 = x0 + s1 + s2
+//   X1, X4 = x0 + c1 s1 + c2 s2 -+ i (s1' d1 + s2' d2)
+//   X2, X3 = x0 + c2 s1 + c1 s2 -+ i (s2' d1 - s1' d2)
+// (forward: the upper signs, e^{-2 pi i/5}; inverse: the lower).  Constants
+// are cos/sin of 2 pi/5 and 4 pi/5 rounded to double.
+template <bool INV>
+__device__ __forceinline__ void dft5(double2 &x0, double2 &x1, double2 &x2, double2 &x3, double2 &x4) {
+  constexpr double C1 = 0.30901699437494745, C2 = -0.8090169943749475;
+  constexpr double S1 = 0.9510565162951535, S2 = 0.5877852522924731;
+  const double2 s1 = cadd(x1, x4), d1 = csub(x1, x4), s2 = cadd(x2, x3), d2 = csub(x2, x3);
+  const double2 t1 = make_double2(fma(C2, s2.x, fma(C1, s1.x, x0.x)), fma(C2, s2.y, fma(C1, s1.y, x0.y)));
+  const double2 t2 = make_double2(fma(C1, s2.x, fma(C2, s1.x, x0.x)), fma(C1, s2.y, fma(C2, s1.y, x0.y)));
+  // u = S1 d1 + S2 d2, v = S2 d1 - S1 d2 (real combinations), then times -i (forward) or +i
+  const double2 u = make_double2(fma(S2, d2.x, S1 * d1.x), fma(S2, d2.y, S1 * d1.y));
+  const double2 v = make_double2(fma(-S1, d2.x, S2 * d1.x), fma(-S1, d2.y, S2 * d1.y));
+  const double2 iu = cmul_mi<INV>(u), iv = cmul_mi<INV>(v);
+  x0 = cadd(x0, cadd(s1, s2));
+  x1 = cadd(t1, iu);
+  x4 = csub(t1, iu);
+  x2 = cadd(t2, iv);
+  x3 = csub(t2, iv);
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dftR(double2 *x) {
   if constexpr (R == 2) dft2<INV>(x[0], x[1]);
   else if constexpr (R == 4) dft4<INV>(x[0], x[1], x[2], x[3]);
   else if constexpr (R == 8) dft8<INV>(x);
   else if constexpr (R == 3) dft3<INV>(x[0], x[1], x[2]);
+  else if constexpr (R == 5) dft5<INV>(x[0], x[1], x[2], x[3], x[4]);
 }
 
 // ------------------------------------------------------------------ block FFT
@@ -148,8 +174,10 @@ template <int N> struct GroupSync {
 constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x / 2); }
 
 template <int L> struct Radices {
-  static constexpr bool has3 = (L % 3) == 0;
-  static constexpr int L2 = has3 ? L / 3 : L;        // power of two part
+  // odd factor of L (3 or 5), done as a first stage from shared memory
+  static constexpr int F = (L % 3) == 0 ? 3 : ((L % 5) == 0 ? 5 : 1);
+  static constexpr bool has3 = F != 1;  // an odd first stage (radix 3 or 5)
+  static constexpr int L2 = L / F;       // power of two part
   static constexpr int log2L2 = ilog2(L2);
   static constexpr int n8 = log2L2 / 3;               // radix-8 stages
   static constexpr int rem = 1 << (log2L2 % 3);       // 1, 2 or 4
@@ -176,7 +204,7 @@ template <int L, int W> struct TileSmem {
 // which is conflict-free already (and coalesced from global memory).
 template <int L> struct StagedTw {
   using RX = Radices<L>;
-  static constexpr int NS0 = RX::has3 ? 3 : 1;
+  static constexpr int NS0 = RX::F;
   __host__ __device__ static constexpr int offset(int NS) {
     int off = 0, ns = NS0;
     for (int k = 0; k < RX::n8; k++, ns *= 8) {
@@ -298,20 +326,22 @@ __device__ __forceinline__ void store_regs(const double2 (&v)[PTS], int t, int s
   for (int i = 0; i < PTS; i++) sm[sidx<L, W>(t + i * TC, s)] = v[i];
 }
 
-// Radix-3 first stage (NS = 1, no twiddles) run from shared memory: the L/3
-// butterflies of each column are spread over the column's L/8 threads.
+// Odd first stage (radix F = 3 or 5, NS = 1, no twiddles) run from shared
+// memory: the L/F butterflies of each column are spread over the column's
+// L/8 threads.
 template <int L, int W, bool INV, class Sync>
-__device__ __forceinline__ void smem_radix3_stage(int t, int s, double2 *sm, const Sync &sync) {
-  constexpr int TC = L / PTS, NB = L / 3;
+__device__ __forceinline__ void smem_odd_stage(int t, int s, double2 *sm, const Sync &sync) {
+  constexpr int F = Radices<L>::F;
+  constexpr int TC = L / PTS, NB = L / F;
   constexpr int MAXB = (NB + TC - 1) / TC;
-  double2 a[MAXB][3];
+  double2 a[MAXB][F];
 #pragma unroll
   for (int q = 0; q < MAXB; q++) {
     const int j = t + q * TC;
     if (j < NB) {
 #pragma unroll
-      for (int r = 0; r < 3; r++) a[q][r] = sm[sidx<L, W>(j + r * NB, s)];
-      dft3<INV>(a[q][0], a[q][1], a[q][2]);
+      for (int r = 0; r < F; r++) a[q][r] = sm[sidx<L, W>(j + r * NB, s)];
+      dftR<F, INV>(a[q]);
     }
   }
   sync();
@@ -320,7 +350,7 @@ __device__ __forceinline__ void smem_radix3_stage(int t, int s, double2 *sm, con
     const int j = t + q * TC;
     if (j < NB) {
 #pragma unroll
-      for (int r = 0; r < 3; r++) sm[sidx<L, W>(3 * j + r, s)] = a[q][r];
+      for (int r = 0; r < F; r++) sm[sidx<L, W>(F * j + r, s)] = a[q][r];
     }
   }
   sync();
@@ -359,10 +389,10 @@ __device__ __forceinline__ void block_fft(double2 (&v)[PTS], int t, int s, doubl
   if constexpr (RX::has3) {
     store_regs<L, W>(v, t, s, sm);
     sync();
-    smem_radix3_stage<L, W, INV>(t, s, sm, sync);
+    smem_odd_stage<L, W, INV>(t, s, sm, sync);
     load_regs<L, W>(v, t, s, sm);
     sync();
-    run_pow2_stages<L, W, INV, 3, 0, STAGED>(v, t, s, sm, tw, sync);
+    run_pow2_stages<L, W, INV, RX::F, 0, STAGED>(v, t, s, sm, tw, sync);
   } else {
     run_pow2_stages<L, W, INV, 1, 0, STAGED>(v, t, s, sm, tw, sync);
   }

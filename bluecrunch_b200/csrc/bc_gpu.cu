@@ -43,8 +43,11 @@ struct Shape {
   int M = 0, L1 = 0, L2 = 1, Lr = 1, levels = 0;
 };
 
-constexpr int kRowLens[] = {128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096};
-constexpr int kSmallLens[] = {256, 512, 768, 1024, 1536, 2048, 3072, 4096};
+// Transform lengths are 2^k, 3*2^k and 5*2^k: the odd factor lives in the
+// row length (or the one-CTA length), the outer and middle lengths are
+// powers of two.
+constexpr int kRowLens[] = {128, 192, 256, 320, 384, 512, 640, 768, 1024, 1280, 1536, 2048, 2560, 3072, 4096};
+constexpr int kSmallLens[] = {256, 512, 768, 1024, 1280, 1536, 2048, 2560, 3072, 4096, 5120};
 constexpr int kOuterLens[] = {64, 128, 256, 512};
 constexpr size_t kMaxM = size_t(1) << 30;
 
@@ -58,9 +61,9 @@ size_t pow2part(size_t x) { return x & (~x + 1); }
 // replace it by a tuned one with the same number of levels).
 bool shape_default(size_t M, Shape &s) {
   if (M < 256 || M > kMaxM) return false;
-  const size_t p2 = (M % 3 == 0) ? M / 3 : M;
+  const size_t p2 = (M % 3 == 0) ? M / 3 : ((M % 5 == 0) ? M / 5 : M);
   if (p2 & (p2 - 1)) return false;
-  if (M <= 4096) {
+  if (M <= 5120) {
     for (int x : kSmallLens)
       if ((size_t)x == M) { s.M = (int)M; s.L1 = (int)M; s.L2 = 1; s.Lr = 1; s.levels = 1; return true; }
     return false;
@@ -74,7 +77,7 @@ bool shape_default(size_t M, Shape &s) {
   }
   // three levels: rows of about 1024 points keep the fused row pass free of
   // spills with two rows per CTA; longer rows only when the outer passes run out
-  static const int kRowPref[] = {1024, 768, 1536, 512, 2048, 3072, 4096};
+  static const int kRowPref[] = {1024, 768, 1536, 512, 2048, 3072, 4096, 1280, 640, 2560};
   for (int Lri : kRowPref) {
     const size_t Lr = (size_t)Lri;
     if (M % Lr) continue;
@@ -98,6 +101,7 @@ const std::vector<size_t> &lengths() {
       Shape s;
       if (shape_default(p, s)) r.push_back(p);
       if (3 * p / 2 <= kMaxM && shape_default(3 * p / 2, s)) r.push_back(3 * p / 2);
+      if (5 * p / 4 <= kMaxM && shape_default(5 * p / 4, s)) r.push_back(5 * p / 4);
     }
     std::sort(r.begin(), r.end());
     return r;
@@ -225,6 +229,10 @@ int width_limit(size_t M) {
   if (it != g.width_override.end()) return it->second;
   it = g.width_file.find(M);
   if (it != g.width_file.end()) return it->second;
+  // a length the table does not hold takes the width of the next longer one
+  // it does (the limit only falls with the length)
+  it = g.width_file.upper_bound(M);
+  if (it != g.width_file.end()) return std::min(it->second, default_width_limit(M) + 4);
   return default_width_limit(M);
 }
 
@@ -528,8 +536,8 @@ KInfo get_rows(int L, bool sq) {
     return k;
   }
   switch (L) {
-    ROWCASE(128) ROWCASE(192) ROWCASE(256) ROWCASE(384) ROWCASE(512) ROWCASE(768)
-    ROWCASE(1024) ROWCASE(1536) ROWCASE(2048) ROWCASE(3072) ROWCASE(4096)
+    ROWCASE(128) ROWCASE(192) ROWCASE(256) ROWCASE(320) ROWCASE(384) ROWCASE(512) ROWCASE(640) ROWCASE(768)
+    ROWCASE(1024) ROWCASE(1280) ROWCASE(1536) ROWCASE(2048) ROWCASE(2560) ROWCASE(3072) ROWCASE(4096)
   }
   return {};
 }
@@ -537,8 +545,8 @@ KInfo get_rows(int L, bool sq) {
   case L: return sq ? small_info<L, true>() : small_info<L, false>();
 KInfo get_small(int M, bool sq) {
   switch (M) {
-    SMALLCASE(256) SMALLCASE(512) SMALLCASE(768) SMALLCASE(1024) SMALLCASE(1536) SMALLCASE(2048)
-    SMALLCASE(3072) SMALLCASE(4096)
+    SMALLCASE(256) SMALLCASE(512) SMALLCASE(768) SMALLCASE(1024) SMALLCASE(1280) SMALLCASE(1536) SMALLCASE(2048)
+    SMALLCASE(2560) SMALLCASE(3072) SMALLCASE(4096) SMALLCASE(5120)
   }
   return {};
 }

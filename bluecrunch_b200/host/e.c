@@ -279,10 +279,14 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   }
   /* the GPU engine first, in a phase of its own: opening the device (driver
    * and context start) takes from under one to several seconds on a fresh
-   * process, and would otherwise land in the first phase that multiplies */
-  task_start(1, "Starting GPU engine");
-  bc_host_ensure_gpu();
-  task_end(1);
+   * process, and would otherwise land in the first phase that multiplies.
+   * Below 100 limbs every product stays on the host (as in the reference),
+   * and the engine starts only if one is needed after all. */
+  if (p >= 100) {
+    task_start(1, "Starting GPU engine");
+    bc_host_ensure_gpu();
+    task_end(1);
+  }
   task_start(1, "Summing");
   bigfloat_t P, Q;
   bigfloat_new(P);

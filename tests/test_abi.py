@@ -55,12 +55,19 @@ def test_plans_fit_and_are_exact_sized(n):
         assert p["L1"] * p["L2"] * max(p["Lr"], 1) == M
 
 
-def test_lengths_are_2k_or_3x2k():
+def test_lengths_are_2k_3x2k_5x2k():
     L = bc.lengths()
     assert L == sorted(L) and L[0] == 256 and L[-1] == 1 << 30
     for M in L:
-        m = M // 3 if M % 3 == 0 else M
+        m = M // 3 if M % 3 == 0 else (M // 5 if M % 5 == 0 else M)
         assert m & (m - 1) == 0
+    # every 2^k; 5*2^k from 1280 on except 10240 (no split: a 160-point row is
+    # not whole 8-line swizzle atoms, 1280 threads are too many for the
+    # one-CTA kernel)
+    for k in range(8, 31):
+        assert (1 << k) in L, k
+    for k in range(8, 28):
+        assert ((5 << k) in L) == ((5 << k) != 10240), k
 
 
 def test_width_table_monotone():

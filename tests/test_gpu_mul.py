@@ -161,6 +161,38 @@ def test_shared_b_transform(gpu, orc, bl, als):
         assert orc.modcheck(got_o, other, b, 4) and orc.modcheck(got_s, b, b, 4)
 
 
+@pytest.mark.parametrize("M", [1280, 2560, 5120, 20480, 40960, 163840, 5 << 18, 5 << 20, 5 << 22])
+@pytest.mark.parametrize("kind", ["product", "square", "unbalanced"])
+def test_lengths_with_factor_five(gpu, orc, M, kind):
+    # transform lengths 5*2^k (a radix-5 first stage in the row or one-CTA
+    # transform) between 2^k and 3*2^k; each forced at its width limit
+    b = gpu.width_limit(M)
+    n = (M * b) // 32 - 3
+    a = limbs(M + 1, n)
+    bb = a if kind == "square" else limbs(M + 2, n if kind == "product" else n // 3)
+    gpu.force_plan(M, b)
+    try:
+        c, st = gpu.mul(a, None if kind == "square" else bb, CL=a.size + bb.size, square=kind == "square",
+                        want_stats=True)
+    finally:
+        gpu.force_plan(0, 0)
+    assert st["fft_points"] == M and st["max_round_err"] < 0.25, st
+    if a.size + bb.size <= 1 << 21:
+        assert np.array_equal(c, orc.ntt_mul(a, bb, a.size + bb.size)), (M, kind)
+    else:
+        assert orc.modcheck(c, a, bb, 4), (M, kind)
+
+
+@pytest.mark.parametrize("al,bl", [(1 << 21, 1 << 19), (1 << 22, 1 << 20)])
+def test_unbalanced_product_takes_a_five_length(gpu, orc, al, bl):
+    # 1:4 products: CL = 1.25 * AL fits 5*2^k points, between the 2^(k+2)
+    # that is too short and the 3*2^(k+1) the 2^k / 3*2^k lengths would take
+    a, b = limbs(al + 1, al), limbs(bl + 2, bl)
+    c, st = gpu.mul(a, b, want_stats=True)
+    assert st["fft_points"] % 5 == 0, st
+    assert orc.modcheck(c, a, b, 4)
+
+
 @pytest.mark.parametrize("n", [100, 2048, 30000, 1 << 18, 1 << 20])
 def test_squaring(gpu, orc, n):
     a = limbs(n + 23, n)
