@@ -90,7 +90,11 @@ import oracle
 from conftest import limbs
 bc.init(0)
 R = oracle.restated()
-# M = 2^22 (64 x 64 x 1024), 2^23 (128 x 64 x 1024), 2^24 (128 x 128 x 1024)
+# M = 2^22 (64 x 64 x 1024), 2^23 (128 x 64 x 1024), 2^24 (128 x 128 x 1024):
+# splits with 1024-point rows, which the fused kernel covers (the tuned
+# table may prefer others)
+for M, L1, L2 in ((1 << 22, 64, 64), (1 << 23, 128, 64), (1 << 24, 128, 128)):
+    bc.set_shape(M, L1, L2, 1024)
 for n in (1 << 21, 1 << 22, 1 << 23):
     a, b = limbs(n + 1, n), limbs(n + 2, n)
     c, st = bc.mul(a, b, CL=2 * n, want_stats=True)
