@@ -26,7 +26,7 @@ BC_OK = 0
 ERRORS = {
     -1: "BC_ERR_INVALID", -2: "BC_ERR_NOMEM", -3: "BC_ERR_CUDA", -4: "BC_ERR_TIMEOUT",
     -5: "BC_ERR_PRECISION", -6: "BC_ERR_NOT_INIT", -7: "BC_ERR_TOO_LARGE",
-    -8: "BC_ERR_NO_DEVICE", -9: "BC_ERR_CARRY",
+    -8: "BC_ERR_NO_DEVICE", -9: "BC_ERR_CARRY", -10: "BC_ERR_IO",
 }
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -87,6 +87,10 @@ GPU_SYMBOLS = {
     "bc_gpu_e_series": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
                                        ctypes.POINTER(_sz), ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
                                        ctypes.POINTER(_sz)]),
+    "bc_gpu_decimal_write": (ctypes.c_int, [ctypes.c_void_p, _sz, _sz, _sz, ctypes.c_int, ctypes.c_longlong]),
+    "bc_gpu_device_alloc": (ctypes.c_int, [_sz, ctypes.POINTER(ctypes.c_void_p)]),
+    "bc_gpu_device_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "bc_gpu_copy": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _sz]),
     "bc_gpu_set_stream": (ctypes.c_int, [ctypes.c_void_p]),
     "bc_gpu_plan": (ctypes.c_int, [_sz, _sz, _sz, ctypes.c_int, ctypes.POINTER(PlanInfo)]),
     "bc_gpu_width_limit": (ctypes.c_int, [_sz]),
@@ -197,6 +201,16 @@ def mul_batch(items, want_stats=False):
     if want_stats:
         return outs, {k: getattr(st, k) for k, _ in BatchStats._fields_}
     return outs
+
+
+def decimal_write(limbs, top, n, maxbytes, fd, offset=0):
+    """Nine decimal characters per limb for limbs[top], limbs[top-1], ...,
+    limbs[top-n+1], cut at maxbytes bytes, written at byte `offset` of the
+    open file descriptor fd (bc_gpu_decimal_write).  limbs: numpy uint32 or
+    a CUDA tensor (device memory)."""
+    p, _, keep = _ptr_len(limbs)
+    _check(_lib().bc_gpu_decimal_write(p, top, n, maxbytes, fd, offset), "bc_gpu_decimal_write")
+    del keep
 
 
 def mul_batch_desc(descs, n):

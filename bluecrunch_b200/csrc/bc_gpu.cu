@@ -23,6 +23,8 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>
+
 #include <cudaTypedefs.h>
 
 #include "bc_gpu.h"
@@ -33,6 +35,7 @@
 #include "bc_arith.cuh"
 #include "bc_pass16.cuh"
 #include "bc_block.cuh"
+#include "bc_text.cuh"
 
 using namespace bc;
 
@@ -1676,9 +1679,13 @@ int radix_tree_core(const uint32_t *dy, size_t ylen, const bc_radix_node *nodes,
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(g.stream));  // mg is rewritten for the next depth
   }
-  // the root's digits
-  std::vector<SpanJob> jobs{{0, (char *)out, nodes[0].k * 4}};
-  if ((r = stage_d2h((const char *)(dsd + s_off[0]), jobs, nodes[0].k * 4))) return r;
+  // the root's digits: to the caller's device array, or through the ring
+  if (is_device_ptr(out)) {
+    CK(cudaMemcpyAsync(out, dsd + s_off[0], nodes[0].k * 4, cudaMemcpyDeviceToDevice, g.stream));
+  } else {
+    std::vector<SpanJob> jobs{{0, (char *)out, nodes[0].k * 4}};
+    if ((r = stage_d2h((const char *)(dsd + s_off[0]), jobs, nodes[0].k * 4))) return r;
+  }
   CK(cudaStreamSynchronize(g.stream));
   return BC_OK;
 }
@@ -2269,6 +2276,85 @@ int e_series_locked(uint32_t a, uint32_t b, uint32_t **hP, size_t *PL, uint32_t 
   return BC_OK;
 }
 
+// ------------------------------------------------------------------ decimal text
+// pwrite of [buf, buf + len) at file offset off, in pieces of at least 4 MiB
+// on up to copy_threads() threads (the copy into the page cache is most of
+// the time of a large write).
+int par_pwrite(int fd, const char *buf, size_t len, long long off) {
+  const unsigned nt = (unsigned)std::min<size_t>(copy_threads(), len / (size_t(4) << 20) + 1);
+  const size_t piece = (len + nt - 1) / nt;
+  std::atomic<int> bad{0};
+  auto worker = [&](unsigned k) {
+    size_t o = (size_t)k * piece;
+    const size_t end = std::min(len, o + piece);
+    while (o < end) {
+      const ssize_t w = pwrite(fd, buf + o, end - o, (off_t)(off + (long long)o));
+      if (w <= 0) {
+        bad = 1;
+        return;
+      }
+      o += (size_t)w;
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned k = 1; k < nt; k++) th.emplace_back(worker, k);
+  worker(0);
+  for (std::thread &t : th) t.join();
+  return bad ? fail(BC_ERR_IO) : BC_OK;
+}
+
+// Nine decimal characters per limb for limbs[top], limbs[top-1], ...,
+// limbs[top-n+1], cut at maxbytes, written at file offset off.  The text is
+// rendered in device memory (k_decimal_text) and leaves through the pinned
+// ring, each chunk written by several threads while the next one crosses.
+int decimal_write_locked(const uint32_t *limbs, size_t top, size_t n, size_t maxbytes, int fd, long long off) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (fd < 0 || off < 0 || (n && (!limbs || top + 1 < n)) || n > (SIZE_MAX / 9)) return fail(BC_ERR_INVALID);
+  const size_t bytes = std::min(maxbytes, 9 * n);
+  if (!bytes) return BC_OK;
+  const size_t nl = (bytes + 8) / 9;  // limbs whose text is written, whole or in part
+  DevBuf din, dtext;
+  int r;
+  const uint32_t *dl = limbs;
+  size_t dtop = top;
+  if (!is_device_ptr(limbs)) {  // the nl limbs the text needs, limbs[top-nl+1 .. top]
+    if ((r = din.alloc(nl * 4))) return r;
+    std::vector<SpanJob> jobs{{0, (char *)(limbs + (top + 1 - nl)), nl * 4}};
+    if ((r = stage_h2d((char *)din.p, jobs, nl * 4))) return r;
+    dl = (const uint32_t *)din.p;
+    dtop = nl - 1;
+  }
+  if ((r = dtext.alloc((9 * nl + 15) & ~size_t(15)))) return r;
+  const unsigned long long blocks = (nl + TEXT_LIMBS - 1) / TEXT_LIMBS;
+  if (blocks > 0x7fffffffULL) return fail(BC_ERR_TOO_LARGE);
+  k_decimal_text<<<(unsigned)blocks, TEXT_THREADS, 0, g.stream>>>(dl, dtop, nl, (char *)dtext.p);
+  CK(cudaGetLastError());
+  if ((r = ring_ready())) return r;
+  for (int h = 0; h < 2; h++)
+    if (g_ring.pending[h]) { CK(cudaEventSynchronize(g_ring.ev[h])); g_ring.pending[h] = false; }
+  const char *src = (const char *)dtext.p;
+  const size_t nch = (bytes + kRingChunk - 1) / kRingChunk;
+  auto issue = [&](size_t c) -> int {
+    const int h = (int)(c & 1);
+    const size_t w0 = c * kRingChunk, len = std::min(kRingChunk, bytes - w0);
+    CK(cudaMemcpyAsync(g_ring.half[h], src + w0, len, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaEventRecord(g_ring.ev[h], g.stream));
+    return BC_OK;
+  };
+  if ((r = issue(0))) return r;
+  for (size_t c = 0; c < nch; c++) {
+    if (c + 1 < nch && (r = issue(c + 1))) return r;
+    const int h = (int)(c & 1);
+    CK(cudaEventSynchronize(g_ring.ev[h]));
+    const size_t w0 = c * kRingChunk, len = std::min(kRingChunk, bytes - w0);
+    if ((r = par_pwrite(fd, g_ring.half[h], len, off + (long long)w0))) {
+      CK(cudaStreamSynchronize(g.stream));  // the next chunk's copy is still in flight
+      return r;
+    }
+  }
+  return BC_OK;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -2425,6 +2511,43 @@ int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *n
                           uint32_t *out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   return radix_tree_pow_locked(y, ylen, nodes, nnodes, t0, t0len, steps, ntable, alpha, out);
+}
+
+int bc_gpu_decimal_write(const uint32_t *limbs, size_t top, size_t n, size_t maxbytes, int fd, long long offset) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return decimal_write_locked(limbs, top, n, maxbytes, fd, offset);
+}
+
+int bc_gpu_device_alloc(size_t bytes, void **p) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (!p) return fail(BC_ERR_INVALID);
+  *p = nullptr;
+  if (cudaMalloc(p, std::max<size_t>(bytes, 256)) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(BC_ERR_NOMEM);
+  }
+  return BC_OK;
+}
+
+int bc_gpu_device_free(void *p) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!p) return BC_OK;
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  CK(cudaStreamSynchronize(g.stream));
+  CK(cudaFree(p));
+  return BC_OK;
+}
+
+int bc_gpu_copy(void *dst, const void *src, size_t bytes) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (!bytes) return BC_OK;
+  if (!dst || !src) return fail(BC_ERR_INVALID);
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  return BC_OK;
 }
 
 int bc_gpu_selftest_wait(double *seconds) {
@@ -2595,6 +2718,7 @@ const char *bc_gpu_strerror(int code) {
     case BC_ERR_TOO_LARGE: return "product too large for the supported transform lengths";
     case BC_ERR_NO_DEVICE: return "no sm_100 CUDA device";
     case BC_ERR_CARRY: return "carry out of the top word of an exact product";
+    case BC_ERR_IO: return "writing the output file failed";
   }
   return "unknown error";
 }

@@ -43,4 +43,18 @@ void bc_small_mul(uint32_t *CT, size_t CL, const uint32_t *AT, size_t AL, const 
 uint64_t bc_host_product_check(const uint32_t *C, size_t CL, const uint32_t *A, size_t AL, const uint32_t *B,
                                size_t BL);
 
+/* A binary-to-decimal conversion whose base-10^9 digits stay in device
+ * memory (bigfloat_radix_device): dev holds limbs [0, len) or, when the top
+ * limb was split, [0, len - 1) with the value's top limb in `top`;
+ * value = sum limb[i] 10^(9(i + exp)). */
+typedef struct {
+  uint32_t *dev;
+  size_t len;
+  int64_t exp;
+  uint32_t top;
+} bc_dec_device;
+int bigfloat_radix_device(bc_dec_device *d, const bigfloat_t a);
+int bc_dec_device_write(const bc_dec_device *d, size_t digits, int fd);
+void bc_dec_device_free(bc_dec_device *d);
+
 #endif

@@ -20,7 +20,12 @@
  *
  * The hex digits are formatted and written on a host thread while the
  * radix conversion runs (it only reads e, as the conversion does); the
- * "Writing hex digits" phase reports what is left of it afterwards.
+ * "Writing hex digits" phase reports what is left of it afterwards.  With
+ * the default conversion driver the decimal digits never reach host memory
+ * as numbers: the conversion leaves them in device memory, their text is
+ * rendered there and written to e.txt straight from the pinned staging
+ * buffers (bigfloat_radix_device, bc_dec_device_write), the same bytes as
+ * bigfloat_to_string would give.
  */
 #include <fcntl.h>
 #include <math.h>
@@ -268,6 +273,24 @@ static int dump(const char *dir, const char *name, const char *s, size_t len) {
   return 0;
 }
 
+/* The decimal text of a conversion held in device memory, as dump() would
+ * write bigfloat_to_string's output for it. */
+static int dump_device(const char *dir, const char *name, const bc_dec_device *d, size_t digits) {
+  char path[4096];
+  snprintf(path, sizeof path, "%s/%s", dir ? dir : ".", name);
+  const int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+  if (fd < 0) {
+    fprintf(stderr, "Cannot create file %s\n", path);
+    return -1;
+  }
+  const int bad = bc_dec_device_write(d, digits, fd);
+  if (close(fd) != 0 || bad) {
+    fprintf(stderr, "Cannot write file %s\n", path);
+    return -1;
+  }
+  return 0;
+}
+
 /* main.c:111-167 */
 int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   digits++;  /* the leading 2 does not count */
@@ -321,11 +344,16 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   const int hex_async = pthread_create(&hex_thread, NULL, hex_writer, &hj) == 0;
   if (!hex_async) hex_writer(&hj);
 
+  /* the default conversion leaves its digits in device memory, and their
+   * text is rendered there and written straight from the staging buffers;
+   * the other conversion drivers print on the host */
   task_start(1, "Converting to decimal");
   fflush(stdout);
   bigfloat_t dec;
   bigfloat_new(dec);
-  bigfloat_radix(dec, P);
+  bc_dec_device dd = {NULL, 0, 0, 0};
+  const int on_device = bigfloat_radix_device(&dd, P) == 0;
+  if (!on_device) bigfloat_radix(dec, P);
   task_end(1);
 
   task_start(1, "Writing hex digits");
@@ -334,12 +362,17 @@ int bluecrunch_e(size_t digits, int mode, const char *outdir) {
   task_end(1);
 
   task_start(1, "Writing decimal digits");
-  char *out = (char *)bc_xmalloc(out_len + 22);
-  size_t len = bigfloat_to_string(out, dec, out_len, 10);
-  rc |= dump(outdir, "e.txt", out, len);
+  if (on_device) {
+    rc |= dump_device(outdir, "e.txt", &dd, out_len);
+    bc_dec_device_free(&dd);
+  } else {
+    char *out = (char *)bc_xmalloc(out_len + 22);
+    size_t len = bigfloat_to_string(out, dec, out_len, 10);
+    rc |= dump(outdir, "e.txt", out, len);
+    free(out);
+  }
   bigfloat_free(P);
   bigfloat_free(dec);
-  free(out);
   task_end(1);
   return rc;
 }

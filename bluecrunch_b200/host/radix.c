@@ -22,6 +22,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
+#include <unistd.h>
 
 #include "bc_gpu.h"
 #include "bc_host.h"
@@ -433,7 +434,7 @@ static void convert_levels(bigfloat_t target, size_t k0, const _bigfloat_struct 
  * table's first entry go over once, the digits come back once. */
 static bc_radix_pow_step g_steps[TABLE_SLOTS];
 
-static void convert_tree(bigfloat_t target, size_t k0, const _bigfloat_struct *y0, size_t n0, size_t g) {
+static void convert_tree(uint32_t *out, size_t k0, const _bigfloat_struct *y0, size_t n0, size_t g) {
   double t0 = wall_now();
   size_t cap = 64, nn = 1;
   bc_radix_node *nd = (bc_radix_node *)bc_xmalloc(cap * sizeof(bc_radix_node));
@@ -458,14 +459,13 @@ static void convert_tree(bigfloat_t target, size_t k0, const _bigfloat_struct *y
     nd[nn++] = h;
     nd[nn++] = l;
   }
-  bigfloat_alloc(target, k0);
   bc_host_ensure_gpu();
   int rc;
   if (g_tab.n > 0) {
     rc = bc_gpu_radix_tree_pow(y0->coef, y0->len, nd, nn, g_tab.val[0]->coef, g_tab.val[0]->len, g_steps, g_tab.n,
-                               ALPHA, target->coef);
+                               ALPHA, out);
   } else {
-    rc = bc_gpu_radix_tree(y0->coef, y0->len, nd, nn, NULL, NULL, 0, ALPHA, target->coef);
+    rc = bc_gpu_radix_tree(y0->coef, y0->len, nd, nn, NULL, NULL, 0, ALPHA, out);
   }
   if (rc != BC_OK) {
     fprintf(stderr, "bigfloat_radix: GPU conversion tree of %zu nodes failed: %s\n", nn, bc_gpu_strerror(rc));
@@ -494,7 +494,7 @@ void bigfloat_radix(bigfloat_t target, const bigfloat_t a) {
   task_start(2, "Conversion");
   if (getenv("BC_RADIX_PERCALL")) convert_rec_percall(target, k, a, n, g);
   else if (getenv("BC_RADIX_LEVELS")) convert_levels(target, k, a, n, g);
-  else convert_tree(target, k, a, n, g);
+  else convert_tree(target->coef, k, a, n, g);
   task_end(2);
   table_free(&g_tab);
   if (target->coef[target->len - 1] > NEWBASE) {
@@ -525,52 +525,135 @@ static size_t limb_dec(uint32_t v, char *s) {
   return 9;
 }
 
-/* bigfloat/string.c:62-125, including its choice of how many limbs to print
- * (digits/8 for base 10, digits/9 for base 16) and its final truncation. */
+/* bigfloat/string.c:62-125's layout, including its choice of how many limbs
+ * to print (digits/8 for base 10, digits/9 for base 16) and its final
+ * truncation: after `head` characters ("2." for a value in [1, 2^32), "."
+ * below), the limbs c-1, c-2, ... down to at most c-n, w characters each,
+ * and the length the reference returns, which is how many bytes its caller
+ * writes.  The reference's loop stops after the first limb that brings the
+ * string to `digits` characters; every limb's place is known in advance, so
+ * the limbs can be printed in parallel. */
+typedef struct {
+  size_t head, c, n, w, len;
+} text_plan;
+
+static text_plan plan_text(size_t vlen, int64_t exp, uint32_t top, size_t digits, int base) {
+  text_plan t;
+  const int mag = (int)((int64_t)vlen + exp);
+  t.c = vlen - 1;
+  if (mag == 1 && top != 2) {
+    fprintf(stderr, "Not implemented\n");
+    abort();
+  }
+  t.head = mag == 1 ? 2 : 1;
+  const size_t per = base == 10 ? 8 : 9;
+  const size_t min_c = vlen > digits / per ? vlen - digits / per - 1 : 0;
+  t.w = base == 10 ? 9 : 8;
+  t.n = t.c > min_c ? t.c - min_c : 0;
+  if (t.n) {
+    const size_t need = digits > t.head ? (digits - t.head + t.w - 1) / t.w : 1;
+    if (need < t.n) t.n = need;
+  }
+  const size_t total = t.head + t.n * t.w; /* characters before the terminator */
+  t.len = total + 1 > digits ? digits - 1 : total;
+  return t;
+}
+
 size_t bigfloat_to_string(char *string, const bigfloat_t value, size_t digits, int base) {
-  char *start = string;
   if (value->len == 0) {
     string[0] = '0';
     string[1] = '\0';
     return 1;
   }
-  int mag = (int)((int64_t)value->len + value->exp);
-  size_t c = value->len - 1;
-  if (mag == 1) {
-    if (value->coef[c] != 2) {
-      fprintf(stderr, "Not implemented\n");
-      abort();
-    }
-    *string++ = '2';
-  }
-  *string++ = '.';
-  size_t min_c;
-  size_t per = base == 10 ? 8 : 9;
-  min_c = value->len > digits / per ? value->len - digits / per - 1 : 0;
-  /* The reference's loop (string.c:93-111) emits limbs c-1, c-2, ... down to
-   * min_c, w characters each, and stops after the first limb that brings the
-   * string to `digits` characters.  Every limb's place is known in advance,
-   * so the limbs are written in parallel. */
-  const size_t w = base == 10 ? 9 : 8;
-  const size_t prefix = (size_t)(string - start);
-  const size_t avail = c > min_c ? c - min_c : 0;
-  size_t n = avail;
-  if (n) {
-    const size_t need = digits > prefix ? (digits - prefix + w - 1) / w : 1;
-    if (need < n) n = need;
-  }
-  const long nn = (long)n;
+  const text_plan t = plan_text(value->len, value->exp, value->coef[value->len - 1], digits, base);
+  if (t.head == 2) string[0] = '2';
+  string[t.head - 1] = '.';
+  const long nn = (long)t.n;
 #pragma omp parallel for schedule(static) if (nn > 100000)
   for (long k = 0; k < nn; k++) {
-    const uint32_t v = value->coef[c - 1 - (size_t)k];
-    if (base == 10) limb_dec(v, string + (size_t)k * w);
-    else limb_hex(v, string + (size_t)k * w);
+    const uint32_t v = value->coef[t.c - 1 - (size_t)k];
+    if (base == 10) limb_dec(v, string + t.head + (size_t)k * t.w);
+    else limb_hex(v, string + t.head + (size_t)k * t.w);
   }
-  string += n * w;
-  *string++ = '\0';
-  if ((size_t)(string - start) > digits) {
-    start[digits + 1] = '\0';
-    return digits - 1;
+  const size_t total = t.head + t.n * t.w;
+  string[total] = '\0';
+  if (t.len < total) string[digits + 1] = '\0';
+  return t.len;
+}
+
+/* ---------------------------------------------------------------- decimal text on the device */
+
+/* bigfloat_radix with the default (device tree) driver, leaving the digits
+ * in device memory: the same plan, the same tree, and the same split of a top
+ * limb above 10^9 (bigfloat/radix.c:351-357), whose low part is written back
+ * into the device array.  Returns 0, or -1 when another driver is selected
+ * (BC_RADIX_PERCALL, BC_RADIX_LEVELS), in which case nothing was done. */
+int bigfloat_radix_device(bc_dec_device *d, const bigfloat_t a) {
+  if (getenv("BC_RADIX_PERCALL") || getenv("BC_RADIX_LEVELS")) return -1;
+  if (-a->exp + 1 != (int64_t)a->len) {
+    fprintf(stderr, "Not implemented\n");
+    abort();
   }
-  return (size_t)(string - start) - 1;
+  size_t n = (size_t)(-a->exp);
+  size_t k = (size_t)ceil((double)n * LOGR) - 1;
+  double gd = ceil(log((double)k) / log(OLDBASE)) + 1;
+  size_t g = (size_t)(gd > KT ? gd : KT);
+  task_start(2, "Precomputing base conversion table");
+  table_plan(&g_tab, k, g_steps);
+  task_end(2);
+  task_start(2, "Conversion");
+  bc_host_ensure_gpu();
+  void *dev = NULL;
+  int rc = bc_gpu_device_alloc(k * sizeof(uint32_t), &dev);
+  if (rc != BC_OK) {
+    fprintf(stderr, "bigfloat_radix: %zu limbs of device memory: %s\n", k, bc_gpu_strerror(rc));
+    abort();
+  }
+  convert_tree((uint32_t *)dev, k, a, n, g);
+  task_end(2);
+  table_free(&g_tab);
+  uint32_t top = 0;
+  if ((rc = bc_gpu_copy(&top, (uint32_t *)dev + (k - 1), 4)) != BC_OK) {
+    fprintf(stderr, "bigfloat_radix: %s\n", bc_gpu_strerror(rc));
+    abort();
+  }
+  d->dev = (uint32_t *)dev;
+  d->len = k;
+  if (top > NEWBASE) {
+    const uint32_t lo = top % NEWBASE;
+    if ((rc = bc_gpu_copy((uint32_t *)dev + (k - 1), &lo, 4)) != BC_OK) {
+      fprintf(stderr, "bigfloat_radix: %s\n", bc_gpu_strerror(rc));
+      abort();
+    }
+    top /= NEWBASE;
+    d->len = k + 1;
+  }
+  d->top = top;
+  d->exp = -(int64_t)d->len + 1;
+  return 0;
+}
+
+/* The first bigfloat_to_string(s, value, digits, 10) bytes of the converted
+ * value, written at the start of the open file fd: the head on the host, the
+ * limbs' text rendered on the GPU from the device array
+ * (bc_gpu_decimal_write).  Returns 0, or -1 when writing fails. */
+int bc_dec_device_write(const bc_dec_device *d, size_t digits, int fd) {
+  const text_plan t = plan_text(d->len, d->exp, d->top, digits, 10);
+  const char head[2] = {t.head == 2 ? '2' : '.', '.'};
+  const size_t hl = t.len < t.head ? t.len : t.head;
+  if (hl && pwrite(fd, t.head == 2 ? head : head + 1, hl, 0) != (ssize_t)hl) return -1;
+  if (t.len > t.head) {
+    /* limbs c-1, c-2, ...: all below index len-1, inside the device array */
+    const int rc = bc_gpu_decimal_write(d->dev, t.c - 1, t.n, t.len - t.head, fd, (long long)t.head);
+    if (rc != BC_OK) {
+      fprintf(stderr, "decimal output: %s\n", bc_gpu_strerror(rc));
+      return -1;
+    }
+  }
+  return 0;
+}
+
+void bc_dec_device_free(bc_dec_device *d) {
+  if (d->dev) bc_gpu_device_free(d->dev);
+  d->dev = NULL;
 }

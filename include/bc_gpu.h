@@ -30,7 +30,8 @@ enum {
   BC_ERR_NOT_INIT = -6,    /* bc_gpu_init has not succeeded */
   BC_ERR_TOO_LARGE = -7,   /* product needs a transform longer than supported (2^30 points) */
   BC_ERR_NO_DEVICE = -8,   /* no usable sm_100 device */
-  BC_ERR_CARRY = -9        /* carry out of the top word of an exact product (internal check) */
+  BC_ERR_CARRY = -9,       /* carry out of the top word of an exact product (internal check) */
+  BC_ERR_IO = -10          /* writing an output file failed (bc_gpu_decimal_write) */
 };
 
 /* Configuration for bc_gpu_init; a NULL pointer means all defaults. */
@@ -138,7 +139,9 @@ int bc_gpu_radix_leaves(const bc_radix_leaf *leaves, size_t count, double alpha)
  * child's digit count kl and the index of 10^(9(k-kl)) in `table`; a leaf
  * has child_h = child_l = -1.  Every product, leaf and merge runs in device
  * memory; y and the table entries cross once, the root's k digits come back
- * into out (most significant last).  alpha as for bc_gpu_radix_leaves. */
+ * into out (most significant last; when out is device memory, e.g. from
+ * bc_gpu_device_alloc, they stay on the device).  alpha as for
+ * bc_gpu_radix_leaves. */
 typedef struct {
   size_t k, n;
   long child_h, child_l;
@@ -194,6 +197,25 @@ int bc_gpu_selftest_wait(double *seconds);
 int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *nodes, size_t nnodes,
                           const uint32_t *t0, size_t t0len, const bc_radix_pow_step *steps, int ntable, double alpha,
                           uint32_t *out);
+
+/* Decimal text of base-10^9 limbs, written to an open file: nine
+ * zero-padded characters per limb for limbs[top], limbs[top-1], ...,
+ * limbs[top-n+1] (most significant first, the order of the reference's
+ * printing loop, bigfloat/string.c:93-111), the whole text cut at maxbytes
+ * bytes and placed at byte `offset` of fd (pwrite; the file position is not
+ * used).  limbs may be host or device memory (with bc_gpu_radix_tree_pow
+ * writing its root into a device array, the digits never cross to the host:
+ * the text is rendered on the GPU and leaves through the pinned staging ring,
+ * each chunk written by several threads while the next one crosses).  Each
+ * limb must be below 10^9.  BC_ERR_IO when a write fails. */
+int bc_gpu_decimal_write(const uint32_t *limbs, size_t top, size_t n, size_t maxbytes, int fd, long long offset);
+
+/* Device memory for callers that keep results on the GPU (e.g. the `out` of
+ * bc_gpu_radix_tree_pow, which then stays on the device), and a synchronous
+ * copy between any two host or device ranges. */
+int bc_gpu_device_alloc(size_t bytes, void **p);
+int bc_gpu_device_free(void *p);
+int bc_gpu_copy(void *dst, const void *src, size_t bytes);
 
 /* Launch on this CUDA stream (cudaStream_t as void*; NULL = library stream).
  * Calls still return only when their results are complete. */

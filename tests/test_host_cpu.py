@@ -208,3 +208,49 @@ def test_add_sub_windows_random(seed):
             assert (e, v) == (e_want, want) and s == (1 if full_a > full_b else 0), (case, la, lb, ea, eb, p)
         for q in (x, y, t):
             lib.free(q)
+
+
+def _string_loop(limbs, exp, digits, base):
+    """bigfloat/string.c:62-125 as its sequential loop: head, limbs from the
+    top down to min_c until `digits` characters, then the truncation."""
+    if len(limbs) == 0:
+        return b"0", 1
+    s = bytearray()
+    mag = len(limbs) + exp
+    c = len(limbs) - 1
+    if mag == 1:
+        assert limbs[c] == 2
+        s += b"2"
+    s += b"."
+    per = 8 if base == 10 else 9
+    min_c = len(limbs) - digits // per - 1 if len(limbs) > digits // per else 0
+    while c > min_c:
+        c -= 1
+        s += (b"%09d" % limbs[c]) if base == 10 else (b"%08x" % limbs[c])
+        if len(s) >= digits:
+            break
+    if len(s) + 1 > digits:
+        return bytes(s[:digits - 1]), digits - 1
+    return bytes(s), len(s)
+
+
+def test_to_string_matches_the_sequential_loop():
+    # the layout is computed up front so that limbs print in parallel; it
+    # must reproduce the loop's stopping point and its final truncation for
+    # every length, exponent and digit count, in both bases
+    from bluecrunch_b200.bigfloat import Lib
+    lib = Lib()
+    rng = np.random.default_rng(5)
+    for trial in range(400):
+        n = int(rng.integers(1, 40))
+        base = 10 if trial % 2 else 16
+        lim = rng.integers(0, 10 ** 9 if base == 10 else 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32)
+        exp = -(n - 1) if trial % 3 else -int(rng.integers(n, n + 3))  # integer part 2, or none
+        if exp == -(n - 1):
+            lim[-1] = 2
+        digits = int(rng.integers(1, 9 * n + 30))
+        x = lib.make(lim, exp=exp)
+        got = lib.string(x, digits, base)
+        want, wlen = _string_loop([int(v) for v in lim], exp, digits, base)
+        lib.free(x)
+        assert got == want[:wlen], (n, exp, digits, base)
