@@ -104,41 +104,64 @@ template <int L> struct Pass16 {
   static constexpr int MINB = 384 / NT;
   // dynamic shared memory
   static constexpr size_t TWB = (size_t)L * 16;  // block16 twiddles
-  static constexpr size_t SMEM_INV = 2 * (size_t)L * W * 16 + TWB + (size_t)L * 16 + 1024;
+  static constexpr size_t SMEM_INV = 2 * (size_t)L * W * 16 + TWB + (size_t)L * 16 + 2 * 18 * 16 + 1024;
   static constexpr size_t SMEM_FWD = (size_t)L * W * 16 + (size_t)PackTile<L>::STAGE_WORDS * 4 + TWB +
-                                     (size_t)L * 16 + 1024;
+                                     (size_t)L * 16 + 18 * 16 + 1024;
 };
 
-// Outer-pass twiddles of one thread, e^{-2 pi i col (4 k1 - 1)/(4M)} for
-// k1 = t + R i, as two runs of 8 (base and step from the two-level table,
-// then products; the same accuracy as the 8-point runs).  The table entries
-// are loaded first (OuterRaw16, issued early so their latency overlaps other
-// work) and combined when needed (finish).
-struct OuterRaw16 {
-  double2 l0, h0, l1, h1, ls, hs;
+// Outer-pass twiddles e^{-2 pi i col (4 k1 - 1)/(4M)} of one thread, for
+// k1 = t + R i (i = 0..15) and col = tile W + s, as two runs of 8 (a base
+// and a step, then products).  With T(m) = e^{-2 pi i m/(4M)} (m signed) and
+// T(col x) = T(tile W x) T(s x):
+//   base of the first run   T(col (4t - 1))     = F_t       * T(s (4t - 1))
+//   step                    T(col 4R)           = G         * T(s 4R)
+//   base of the second run  T(col (4t + 32R - 1)) = base1 * H * T(s 32R)
+// The tile factors F_t (t < 16), G = T(tile W 4R), H = T(tile W 32R) are
+// computed once per unit by 18 threads (sincospi) into shared memory; the
+// column factors depend only on the thread (s, t fixed by tid) and stay in
+// registers.  No global twiddle loads remain on the unit's path.
+constexpr int TILE_TW = 18;  // tile factors per unit
+
+// T(m) = e^{-2 pi i m/(4M)} for |m| < 4M: sincospi of m/(2M).
+__device__ __forceinline__ double2 t4m(long long m, double twoM) {
+  double sn, cs;
+  sincospi((double)m / twoM, &sn, &cs);
+  return make_double2(cs, -sn);
+}
+
+struct ColTw16 {
+  double2 c0, cst, cb1;
 };
+template <int R>
+__device__ __forceinline__ ColTw16 col_tw16(int s, int t, double twoM) {
+  ColTw16 c;
+  c.c0 = t4m((long long)s * (4 * t - 1), twoM);
+  c.cst = t4m((long long)s * 4 * R, twoM);
+  c.cb1 = t4m((long long)s * 32 * R, twoM);
+  return c;
+}
+
+// The tile factors of `tile` into fac[0..17], spread over the CTA's warps
+// (a few lanes of each).  The caller's next barrier publishes them.
+template <int R, int W, int NT>
+__device__ __forceinline__ void tile_tw16(double2 *fac, int tile, double twoM) {
+  constexpr int NW = NT / 32, PER = (TILE_TW + NW - 1) / NW;
+  const int lane = threadIdx.x & 31, j = (threadIdx.x >> 5) * PER + lane;
+  if (lane < PER && j < TILE_TW) {
+    const long long tw = (long long)tile * W;
+    const long long x = j < 16 ? 4 * j - 1 : (j == 16 ? 4 * R : 32 * R);
+    fac[j] = t4m(tw * x, twoM);
+  }
+}
+
 struct OuterRun16 {
   double2 b0, b1, st;
 };
-template <int R>
-__device__ __forceinline__ OuterRaw16 outer_raw16(const Tw2 &T, int col, int t) {
-  const uint64_t m0 = t == 0 ? (uint64_t)col : (uint64_t)col * (uint64_t)(4 * t - 1);
-  const uint64_t m1 = (uint64_t)col * (uint64_t)(4 * (t + 8 * R) - 1), ms = (uint64_t)col * (uint64_t)(4 * R);
-  OuterRaw16 r;
-  r.l0 = __ldg(&T.lo[m0 & T.mask]);
-  r.h0 = __ldg(&T.hi[m0 >> T.h]);
-  r.l1 = __ldg(&T.lo[m1 & T.mask]);
-  r.h1 = __ldg(&T.hi[m1 >> T.h]);
-  r.ls = __ldg(&T.lo[ms & T.mask]);
-  r.hs = __ldg(&T.hi[ms >> T.h]);
-  return r;
-}
-__device__ __forceinline__ OuterRun16 outer_finish16(const OuterRaw16 &r, int t) {
+__device__ __forceinline__ OuterRun16 outer_run16(const double2 *fac, const ColTw16 &c, int t) {
   OuterRun16 o;
-  o.b0 = cmul(r.l0, r.h0);
-  if (t == 0) o.b0.y = -o.b0.y;  // k1 = 0: e^{+2 pi i col/(4M)}
-  o.b1 = cmul(r.l1, r.h1);
-  o.st = cmul(r.ls, r.hs);
+  o.b0 = cmul(fac[t], c.c0);
+  o.st = cmul(fac[16], c.cst);
+  o.b1 = cmul(o.b0, cmul(fac[17], c.cb1));
   return o;
 }
 
@@ -157,9 +180,12 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB) k3_outer_fwd(C
   uint32_t *stg = reinterpret_cast<uint32_t *>(tile + L * W);  // one stage of STAGE_WORDS
   double2 *twS = reinterpret_cast<double2 *>(stg + K::STAGE_WORDS);
   double2 *pwS = twS + L;
+  double2 *fac = pwS + L;  // tile factors of the current unit
   tw16_build<L>(twS, p.twL1);
   table_to_smem(pwS, p.pw_fwd, L);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const double twoM = 2.0 * (double)p.M;
+  const ColTw16 ct = col_tw16<R>(s, t, twoM);
   const int tiles = p.S1 / W;
   const unsigned nA = fwd_units_a(p, (unsigned)tiles);
   const unsigned total = nA + fwd_units_b(p, (unsigned)tiles);  // far below 2^32
@@ -210,10 +236,9 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB) k3_outer_fwd(C
     const int tl = (int)f.rest, op = f.op;
     const ItemDesc &it = p.items[f.item];
     const int col = tl * W + s;
-    // twiddle table loads first: their latency overlaps the digits and the transform
-    const OuterRaw16 twr = outer_raw16<R>(p.tw4M, col, t);
     cp_async_wait<0>();
-    __syncthreads();  // the stage (every thread's copies) has landed
+    __syncthreads();  // the stage (every thread's copies) has landed; the last unit's factors are read
+    tile_tw16<R, W, NT>(fac, tl, twoM);  // read after block16's barriers
     const unsigned nd = (unsigned)(op ? it.ndB : it.ndA);  // below 2^30
     double2 *gbuf = op ? it.bufB : it.bufA;
     const int b = it.b;
@@ -252,7 +277,7 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB) k3_outer_fwd(C
     if (un < total) stage_copy(un);
     cp_async_commit();
     block16<L, W, false>(v, t, s, tile, twS);
-    const OuterRun16 tw = outer_finish16(twr, t);
+    const OuterRun16 tw = outer_run16(fac, ct, t);
     double2 w = tw.b0;
 #pragma unroll
     for (int i = 0; i < P16; i++) {
@@ -276,12 +301,16 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
   double2 *const buf0 = align1024(smraw);  // stage st's tile at buf0 + st * L * W
   double2 *twS = buf0 + 2 * L * W;
   double2 *pwS = twS + L;
+  double2 *fac = pwS + L;  // tile factors of unit parity st at fac + st * TILE_TW
   tw16_build<L>(twS, p.twL1);
   table_to_smem(pwS, p.pw_inv, L);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
   const unsigned tiles = p.S1 / W;
   const unsigned total = (unsigned)p.nitems * tiles;  // far below 2^32
   const FastDiv fd_tiles(tiles);
+  const double twoM = 2.0 * (double)p.M;
+  const ColTw16 ct = col_tw16<R>(s, t, twoM);
+  if (blockIdx.x < total) tile_tw16<R, W, NT>(fac, (int)(blockIdx.x % tiles), twoM);
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -305,15 +334,13 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
     }
     const int item = (int)fd_tiles.div(u), tile = (int)(u - (unsigned)item * tiles);
     const ItemDesc &it = p.items[item];
-    const int col = tile * W + s;
-    const OuterRaw16 twr = outer_raw16<R>(p.tw4M, col, t);  // global loads, before the wait
     const unsigned par = (phases >> st) & 1u;
     const bool ok = mbar_wait(&bars[st], par);
     phases ^= 1u << st;
     double2 *bf = buf0 + st * L * W;
     double2 v[P16];
     {
-      const OuterRun16 tw = outer_finish16(twr, t);
+      const OuterRun16 tw = outer_run16(fac + st * TILE_TW, ct, t);
       double2 w = tw.b0;
 #pragma unroll
       for (int i = 0; i < P16; i++) {
@@ -330,6 +357,8 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
       }
       return;
     }
+    // the next unit's tile factors (read after this unit's last barrier)
+    if (un < total) tile_tw16<R, W, NT>(fac + (st ^ 1) * TILE_TW, (int)(un % tiles), twoM);
     block16<L, W, true>(v, t, s, bf, twS);
     double err = 0.0;
 #pragma unroll
