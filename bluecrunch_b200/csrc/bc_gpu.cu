@@ -144,6 +144,10 @@ struct Ctx {
   // copy_stream, so the outer pass packs the first operand meanwhile
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t copy_ev[2] = {nullptr, nullptr};
+  // the classes of a batch run on these streams side by side (they share no
+  // data): a small class's kernels fill the SMs a large one leaves idle
+  cudaStream_t class_stream[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t class_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // [4]: fork
   std::vector<std::pair<const char *, double>> ktimes;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;
@@ -1302,9 +1306,23 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   const int *down = (const int *)((const char *)ddesc + align256(nw * sizeof(ItemDesc)));
   unsigned int *ctr = (unsigned int *)(base + off_ctr);
 
-  // ---- launches
+  // ---- launches: one class after another on the library stream, or, for
+  // several classes, round robin over the class streams (forked from and
+  // joined back into the library stream).  Per-kernel timing and the
+  // cooperative fused kernel keep the single stream.
   pt.next(&g_prof.launch);
   CK(cudaEventRecord(g.ev0, g.stream));
+  const int nstreams = (classes.size() > 1 && !g.time_kernels && !g.fused && !b_late)
+                           ? (int)std::min<size_t>(classes.size(), 4) : 0;
+  if (nstreams) {
+    for (int k = 0; k < 5; k++)
+      if (!g.class_ev[k]) CK(cudaEventCreateWithFlags(&g.class_ev[k], cudaEventDisableTiming));
+    CK(cudaEventRecord(g.class_ev[4], g.stream));
+    for (int k = 0; k < nstreams; k++) {
+      if (!g.class_stream[k]) CK(cudaStreamCreateWithFlags(&g.class_stream[k], cudaStreamNonBlocking));
+      CK(cudaStreamWaitEvent(g.class_stream[k], g.class_ev[4], 0));
+    }
+  }
   size_t first = 0, cls = 0;
   for (auto &c : classes) {
     const size_t n = c.second.size();
@@ -1331,12 +1349,17 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     for (size_t k = first; k < first + n; k++) tiles += works[order[k]]->pl.ntiles;
     p.carry_tiles = tiles;
     const ClassSlab &cs = slab[c.first];
+    cudaStream_t cstream = nstreams ? g.class_stream[cls % nstreams] : g.stream;
     if ((r = launch_class(s, sq, p, (long long)n, tiles, (double2 *)(base + cs.offA),
-                          sq ? nullptr : (double2 *)(base + cs.offB), g.stream, true, &st->launches,
+                          sq ? nullptr : (double2 *)(base + cs.offB), cstream, true, &st->launches,
                           b_late ? g.copy_ev[1] : nullptr)))
       return r;
     first += n;
     cls++;
+  }
+  for (int k = 0; k < nstreams; k++) {
+    CK(cudaEventRecord(g.class_ev[k], g.class_stream[k]));
+    CK(cudaStreamWaitEvent(g.stream, g.class_ev[k], 0));
   }
   CK(cudaEventRecord(g.ev1, g.stream));
   st->classes += classes.size();
@@ -2449,6 +2472,10 @@ int bc_gpu_shutdown(void) {
   if (g.ev1) cudaEventDestroy(g.ev1);
   if (g.own_stream) cudaStreamDestroy(g.own_stream);
   if (g.copy_stream) cudaStreamDestroy(g.copy_stream);
+  for (auto &cs : g.class_stream)
+    if (cs) cudaStreamDestroy(cs);
+  for (auto &e : g.class_ev)
+    if (e) cudaEventDestroy(e);
   for (auto &e : g.copy_ev)
     if (e) cudaEventDestroy(e);
   g_occ.clear();
