@@ -87,6 +87,7 @@ GPU_SYMBOLS = {
     "bc_gpu_e_series": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
                                        ctypes.POINTER(_sz), ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
                                        ctypes.POINTER(_sz)]),
+    "bc_gpu_mul_small_batch": (ctypes.c_int, [ctypes.POINTER(MulDesc), _sz]),
     "bc_gpu_decimal_write": (ctypes.c_int, [ctypes.c_void_p, _sz, _sz, _sz, ctypes.c_int, ctypes.c_longlong]),
     "bc_gpu_device_alloc": (ctypes.c_int, [_sz, ctypes.POINTER(ctypes.c_void_p)]),
     "bc_gpu_device_free": (ctypes.c_int, [ctypes.c_void_p]),
@@ -200,6 +201,25 @@ def mul_batch(items, want_stats=False):
     _check(_lib().bc_gpu_mul_batch(descs, len(items), ctypes.byref(st)), "bc_gpu_mul_batch")
     if want_stats:
         return outs, {k: getattr(st, k) for k, _ in BatchStats._fields_}
+    return outs
+
+
+def mul_small_batch(items):
+    """Exact small products in one launch (bc_gpu_mul_small_batch): items are
+    (a, b, CL_or_None) of numpy uint32 limbs, at most 256 limbs per operand
+    and 512 per product.  Returns the list of outputs."""
+    descs = (MulDesc * max(len(items), 1))()
+    keep, outs = [], []
+    for i, (a, b, CL) in enumerate(items):
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        CL = (a.size + b.size) if CL is None else CL
+        out = np.zeros(max(CL, 1), dtype=np.uint32)
+        keep += [a, b]
+        outs.append(out[:CL])
+        descs[i] = MulDesc(out.ctypes.data, CL, a.ctypes.data, a.size, b.ctypes.data, b.size)
+    _check(_lib().bc_gpu_mul_small_batch(descs, len(items)), "bc_gpu_mul_small_batch")
+    del keep
     return outs
 
 

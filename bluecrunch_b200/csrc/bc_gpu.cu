@@ -36,6 +36,7 @@
 #include "bc_pass16.cuh"
 #include "bc_block.cuh"
 #include "bc_text.cuh"
+#include "bc_school.cuh"
 
 using namespace bc;
 
@@ -2299,6 +2300,66 @@ int e_series_locked(uint32_t a, uint32_t b, uint32_t **hP, size_t *PL, uint32_t 
   return BC_OK;
 }
 
+// ------------------------------------------------------------------ small exact products
+// Products of at most SCHOOL_MAX limbs per operand, from and to host memory:
+// descriptors and operands cross in one staged span, k_school computes all of
+// them (one warp per product), the results come back in one span.
+int mul_small_locked(const bc_mul_desc *items, size_t n) {
+  if (!g.init) return fail(BC_ERR_NOT_INIT);
+  if (n && !items) return fail(BC_ERR_INVALID);
+  std::vector<size_t> live;  // items with both operands nonempty
+  live.reserve(n);
+  for (size_t i = 0; i < n; i++) {
+    const bc_mul_desc &d = items[i];
+    if (d.CL > (size_t)SCHOOL_CMAX || d.AL > (size_t)SCHOOL_MAX || d.BL > (size_t)SCHOOL_MAX)
+      return fail(BC_ERR_TOO_LARGE);
+    if ((d.CL && !d.C) || (d.AL && !d.A) || (d.BL && !d.B)) return fail(BC_ERR_INVALID);
+    if (is_device_ptr(d.C) || (d.AL && is_device_ptr(d.A)) || (d.BL && is_device_ptr(d.B)))
+      return fail(BC_ERR_INVALID);
+    if (d.CL && (!d.AL || !d.BL)) memset(d.C, 0, d.CL * 4);  // a zero operand
+    else if (d.CL) live.push_back(i);
+  }
+  if (live.empty()) return BC_OK;
+  // input span: descriptors, then every live item's A and B; output span: C
+  const size_t m = live.size();
+  std::vector<SchoolDesc> desc(m);
+  const size_t desc_words = align256(m * sizeof(SchoolDesc)) / 4;
+  size_t in_words = desc_words, out_words = 0;
+  std::vector<SpanJob> in_jobs, out_jobs;
+  in_jobs.reserve(2 * m + 1);
+  out_jobs.reserve(m);
+  in_jobs.push_back({0, (char *)desc.data(), m * sizeof(SchoolDesc)});
+  for (size_t k = 0; k < m; k++) {
+    const bc_mul_desc &d = items[live[k]];
+    SchoolDesc &q = desc[k];
+    q.AL = (uint32_t)d.AL;
+    q.BL = (uint32_t)d.BL;
+    q.CL = (uint32_t)d.CL;
+    q.pad = 0;
+    q.a = in_words - desc_words;
+    in_jobs.push_back({in_words * 4, (char *)d.A, d.AL * 4});
+    in_words += d.AL;
+    q.b = in_words - desc_words;
+    in_jobs.push_back({in_words * 4, (char *)d.B, d.BL * 4});
+    in_words += d.BL;
+    q.c = out_words;
+    out_jobs.push_back({out_words * 4, (char *)d.C, d.CL * 4});
+    out_words += d.CL;
+  }
+  DevBuf din, dout;
+  int r;
+  if ((r = din.alloc(in_words * 4)) || (r = dout.alloc(out_words * 4))) return r;
+  if ((r = stage_h2d((char *)din.p, in_jobs, in_words * 4))) return r;
+  const unsigned blocks =
+      (unsigned)std::min<size_t>((m + SCHOOL_WARPS - 1) / SCHOOL_WARPS, (size_t)g.sm_count * 16);
+  k_school<<<blocks, 32 * SCHOOL_WARPS, 0, g.stream>>>((const SchoolDesc *)din.p, (unsigned)m,
+                                                        (const uint32_t *)din.p + desc_words, (uint32_t *)dout.p);
+  CK(cudaGetLastError());
+  if ((r = stage_d2h((const char *)dout.p, out_jobs, out_words * 4))) return r;
+  CK(cudaStreamSynchronize(g.stream));
+  return BC_OK;
+}
+
 // ------------------------------------------------------------------ decimal text
 // pwrite of [buf, buf + len) at file offset off, in pieces of at least 4 MiB
 // on up to copy_threads() threads (the copy into the page cache is most of
@@ -2538,6 +2599,11 @@ int bc_gpu_radix_tree_pow(const uint32_t *y, size_t ylen, const bc_radix_node *n
                           uint32_t *out) {
   std::lock_guard<std::recursive_mutex> lk(g_mu);
   return radix_tree_pow_locked(y, ylen, nodes, nnodes, t0, t0len, steps, ntable, alpha, out);
+}
+
+int bc_gpu_mul_small_batch(const bc_mul_desc *items, size_t n) {
+  std::lock_guard<std::recursive_mutex> lk(g_mu);
+  return mul_small_locked(items, n);
 }
 
 int bc_gpu_decimal_write(const uint32_t *limbs, size_t top, size_t n, size_t maxbytes, int fd, long long offset) {

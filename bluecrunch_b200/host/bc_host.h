@@ -36,6 +36,12 @@ void bc_mul_operands(const _bigfloat_struct *a, const _bigfloat_struct *b, size_
 void bc_host_ensure_gpu(void);
 /* All items on the GPU in one batch; aborts with a message on failure. */
 void bc_host_gpu_batch(bc_gpu_item *items, size_t n);
+/* The batch's small products on the GPU in one launch (no aliasing). */
+void bc_host_gpu_small_batch(bc_gpu_item *items, size_t n);
+/* Below this many small products a batch computes them on host threads. */
+#ifndef BC_SMALL_GPU_MIN
+#define BC_SMALL_GPU_MIN 256
+#endif
 /* Product of small operands on the host (schoolbook), CT may alias. */
 void bc_small_mul(uint32_t *CT, size_t CL, const uint32_t *AT, size_t AL, const uint32_t *BT, size_t BL);
 /* The BC_VERIFY check: 0 when C = A*B modulo two 32-bit primes (or when

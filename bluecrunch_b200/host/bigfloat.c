@@ -458,8 +458,8 @@ void bigfloat_mul_batch(bigfloat_mul_item *items, size_t n) {
   /* 1: operands, targets and which products go to the GPU (serial: cheap) */
   bc_gpu_item *g = (bc_gpu_item *)bc_xmalloc((n ? n : 1) * sizeof(bc_gpu_item));
   bc_operand *ops = (bc_operand *)bc_xmalloc((n ? 2 * n : 2) * sizeof(bc_operand));
-  char *kind = (char *)bc_xmalloc(n ? n : 1);  /* 0 zero, 1 host, 2 gpu */
-  size_t ng = 0;
+  char *kind = (char *)bc_xmalloc(n ? n : 1);  /* 0 zero, 1 host, 2 gpu, 3 gpu small */
+  size_t ng = 0, ns = 0;
   for (size_t i = 0; i < n; i++) {
     _bigfloat_struct *t = items[i].target;
     const _bigfloat_struct *a = items[i].a, *b = items[i].b;
@@ -473,6 +473,7 @@ void bigfloat_mul_batch(bigfloat_mul_item *items, size_t n) {
     const size_t CL = oa->L + ob->L;
     uint32_t *c = (uint32_t *)bc_xmalloc(CL * sizeof(uint32_t));
     kind[i] = (CL == 2 || CL < BC_SMALL_PRODUCT_LIMBS) ? 1 : 2;
+    if (kind[i] == 1 && CL > 2) ns++;
     if (kind[i] == 2) {
       g[ng].C = c; g[ng].CL = CL; g[ng].A = oa->T; g[ng].AL = oa->L; g[ng].B = ob->T; g[ng].BL = ob->L;
       ng++;
@@ -483,12 +484,30 @@ void bigfloat_mul_batch(bigfloat_mul_item *items, size_t n) {
     t->exp = oa->exp + ob->exp;
     t->len = CL;
   }
-  /* 2: GPU products in one batch while host threads do the small ones */
+  /* 2: GPU products in one batch while host threads do the small ones; many
+   * small ones (the lower levels of a level-ordered tree) go to the GPU as
+   * one more batch (schoolbook, one launch) */
+  bc_gpu_item *sg = NULL;
+  if (ns >= BC_SMALL_GPU_MIN) {
+    sg = (bc_gpu_item *)bc_xmalloc(ns * sizeof(bc_gpu_item));
+    ns = 0;
+    for (size_t i = 0; i < n; i++) {
+      if (kind[i] != 1 || items[i].target->len == 2) continue;
+      const bc_operand *oa = &ops[2 * i], *ob = &ops[2 * i + 1];
+      _bigfloat_struct *t = items[i].target;
+      sg[ns].C = t->coef; sg[ns].CL = t->len; sg[ns].A = oa->T; sg[ns].AL = oa->L; sg[ns].B = ob->T; sg[ns].BL = ob->L;
+      ns++;
+      kind[i] = 3;
+    }
+  }
   long nn = (long)n;
 #pragma omp parallel
   {
 #pragma omp single nowait
-    if (ng) bc_host_gpu_batch(g, ng);
+    {
+      if (ng) bc_host_gpu_batch(g, ng);
+      if (sg) bc_host_gpu_small_batch(sg, ns);
+    }
 #pragma omp for schedule(dynamic, 256)
     for (long i = 0; i < nn; i++) {
       if (kind[i] != 1) continue;
@@ -508,6 +527,7 @@ void bigfloat_mul_batch(bigfloat_mul_item *items, size_t n) {
   free(kind);
   free(ops);
   free(g);
+  free(sg);
 }
 
 /* bigfloat/mul.c:64-80: a *= b in place over a->len limbs, the top limb

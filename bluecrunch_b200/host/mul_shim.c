@@ -196,6 +196,29 @@ void bc_host_gpu_batch(bc_gpu_item *items, size_t n) {
     for (size_t i = 0; i < n; i++) verify(items[i].C, items[i].CL, items[i].A, items[i].AL, items[i].B, items[i].BL);
 }
 
+/* Small products (fewer than BC_SMALL_PRODUCT_LIMBS output limbs) of a batch
+ * on the GPU in one launch (bc_gpu_mul_small_batch); aborts with a message on
+ * failure.  C must not alias A or B (bigfloat_mul_batch writes fresh arrays). */
+void bc_host_gpu_small_batch(bc_gpu_item *items, size_t n) {
+  bc_host_ensure_gpu();
+  bc_mul_desc *d = (bc_mul_desc *)bc_xmalloc(n * sizeof(bc_mul_desc));
+  for (size_t i = 0; i < n; i++) {
+    d[i].C = items[i].C; d[i].CL = items[i].CL;
+    d[i].A = items[i].A; d[i].AL = items[i].AL;
+    d[i].B = items[i].B; d[i].BL = items[i].BL;
+  }
+  double t0 = now_s();
+  int rc = bc_gpu_mul_small_batch(d, n);
+  count(n, 1, now_s() - t0);
+  free(d);
+  if (rc != BC_OK) {
+    fprintf(stderr, "bigfloat_mul_batch: GPU batch of %zu small products failed: %s\n", n, bc_gpu_strerror(rc));
+    abort();
+  }
+  if (verify_on())
+    for (size_t i = 0; i < n; i++) verify(items[i].C, items[i].CL, items[i].A, items[i].AL, items[i].B, items[i].BL);
+}
+
 /* Exact schoolbook product of the low CL limbs (the value the reference's
  * _basecase_mul, bigfloat/mul.c:176-220, and _karatzuba_mul, :367-553,
  * produce).  Works through a temporary so CT may alias AT or BT. */

@@ -99,6 +99,15 @@ int bc_gpu_mul(uint32_t *C, size_t CL, const uint32_t *A, size_t AL,
  * bucketed by transform length and every pass covers a whole bucket. */
 int bc_gpu_mul_batch(const bc_mul_desc *items, size_t n, bc_batch_stats *stats);
 
+/* Small products, exact, in one launch: every operand at most 256 limbs and
+ * every C at most 512 limbs (BC_ERR_TOO_LARGE beyond), all arrays in host
+ * memory (BC_ERR_INVALID for device memory).  C = A*B mod 2^(32 CL), zero
+ * above AL + BL limbs.  The reference computes products of this size on the
+ * CPU with its basecase / Karatsuba code (bigfloat/mul.c:176-553, below 100
+ * output limbs, mul.c:640-648); here a batch of them is one schoolbook
+ * kernel (one warp per product, integer column sums, no rounding). */
+int bc_gpu_mul_small_batch(const bc_mul_desc *items, size_t n);
+
 /* Same, with hints: BC_BATCH_HOST_OPERANDS declares every A, B and C to be
  * host memory, BC_BATCH_DEVICE_OPERANDS every one to be device memory (each
  * skips the per-pointer memory query, which dominates batches of millions of
