@@ -32,6 +32,7 @@
 #include "bc_bsr.cuh"
 #include "bc_radix.cuh"
 #include "bc_rows_warp.cuh"
+#include "bc_rows_w512.cuh"
 #include "bc_arith.cuh"
 #include "bc_pass16.cuh"
 #include "bc_block.cuh"
@@ -137,7 +138,7 @@ struct Ctx {
   int last_error = 0;
   int last_cuda = 0;
   bool time_kernels = false;
-  bool rows_warp = true;  // 1024-point rows by k2_rows_w1024 ($BC_ROWS_WARP=0: the block kernel)
+  bool rows_warp = true;  // 512- and 1024-point rows one warp per row ($BC_ROWS_WARP=0: the block kernel)
   bool pass16 = true;     // outer passes of L1 <= 256 with 16 points per thread ($BC_PASS16=0: 8 points)
   bool fused = false;     // three-level middle in one kernel where it applies ($BC_FUSED=1; default: separate passes)
   bool share_b = true;    // one B transform for items with the same device B ($BC_SHARE_B=0: one per item)
@@ -537,6 +538,12 @@ KInfo get_mid(int L, bool inv) {
 #define ROWCASE(L) \
   case L: return sq ? rows_info<L, true>() : rows_info<L, false>();
 KInfo get_rows(int L, bool sq) {
+  if (L == R5_L && g.rows_warp) {
+    KInfo k{sq ? (const void *)k2_rows_w512<true> : (const void *)k2_rows_w512<false>, 32 * R5_WARPS, R5_SMEM,
+            "rows", SIG_P_MAP2};
+    k.warp_rows = true;
+    return k;
+  }
   if (L == RW_L && g.rows_warp) {
     KInfo k{sq ? (const void *)k2_rows_w1024<true> : (const void *)k2_rows_w1024<false>, 32 * RW_WARPS, RW_SMEM,
             "rows", SIG_P_MAP2};
@@ -754,7 +761,8 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
       // one warp per row, plain loads and stores: no tensor maps
       KInfo kr = get_rows(s.Lr, sq);
       const long long rows = n * (long long)(s.M / s.Lr);
-      if ((r = launch(kr, (rows + RW_WARPS - 1) / RW_WARPS, p, nl, stream, timed))) return r;
+      const long long wpc = kr.threads / 32;  // rows (warps) per CTA
+      if ((r = launch(kr, (rows + wpc - 1) / wpc, p, nl, stream, timed))) return r;
     } else {
       KInfo kr = get_rows(s.Lr, sq);
       const int NR = kr.threads / (s.Lr / PTS);
