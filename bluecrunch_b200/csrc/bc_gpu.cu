@@ -705,7 +705,7 @@ KInfo get_fused(int L2, bool sq) {
 // counter and status words zeroed by the caller.
 int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, unsigned long long carry_tiles,
                  double2 *slabA, double2 *slabB, cudaStream_t stream, bool timed, size_t *nl,
-                 cudaEvent_t b_ready = nullptr) {
+                 cudaEvent_t b_ready = nullptr, bool w16 = false) {
   int r;
   if (!shape_launch_ok(s, sq)) return fail(BC_ERR_INVALID);
   if (s.levels == 1) return launch(get_small(s.M, sq), n, p, nl, stream, timed);
@@ -796,7 +796,7 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
     if ((r = encode_map(&oA, slabA, 3, dims, str, box))) return r;
     if ((r = launch(ki, n * (long long)(S1 / W1), p, nl, stream, timed, &oA))) return r;
   }
-  KInfo kc{(const void *)k_carry, CARRY_NT, 0, "carry", SIG_P};
+  KInfo kc{w16 ? (const void *)k_carry<128> : (const void *)k_carry<0>, CARRY_NT, 0, "carry", SIG_P};
   return launch(kc, (long long)carry_tiles, p, nl, stream, timed);
 }
 
@@ -1355,13 +1355,17 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     p.fwd_ops = 0;
     p.slab_elems = align256(s.M * 16) / 16;
     unsigned long long tiles = 0;
-    for (size_t k = first; k < first + n; k++) tiles += works[order[k]]->pl.ntiles;
+    bool w16 = true;  // every item of the class has width 16: the carry pass specialised for it
+    for (size_t k = first; k < first + n; k++) {
+      tiles += works[order[k]]->pl.ntiles;
+      w16 = w16 && works[order[k]]->pl.b == 16;
+    }
     p.carry_tiles = tiles;
     const ClassSlab &cs = slab[c.first];
     cudaStream_t cstream = nstreams ? g.class_stream[cls % nstreams] : g.stream;
     if ((r = launch_class(s, sq, p, (long long)n, tiles, (double2 *)(base + cs.offA),
                           sq ? nullptr : (double2 *)(base + cs.offB), cstream, true, &st->launches,
-                          b_late ? g.copy_ev[1] : nullptr)))
+                          b_late ? g.copy_ev[1] : nullptr, w16)))
       return r;
     first += n;
     cls++;

@@ -280,6 +280,9 @@ __device__ __forceinline__ int rec_chunk_pos(int c) { return (c & ~7) | ((c ^ (c
 // tile's last one, for the word that straddles it).
 constexpr int HC_STRIDE = CARRY_TILE_RUNS + 1;
 
+// NB = 128: every item of the class has width 16 (runs of 128 bits), so the
+// run arithmetic below is specialised at compile time; NB = 0: any width.
+template <int NB>
 __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
   // records of the tile (32 KB), then reused for the corrected values
   __shared__ __align__(16) unsigned long long srec[CARRY_TILE_RUNS * 4];
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
     const unsigned long long rt = tile * CARRY_TILE_RUNS;  // first run of the tile
     const unsigned long long nruns = it.nruns;
     const int nr = (int)min((unsigned long long)CARRY_TILE_RUNS, nruns - rt);  // runs of this tile
-    const int nbits = 8 * it.b;
+    const int nbits = NB ? NB : 8 * it.b;
     const unsigned long long nrec = (unsigned long long)(2 * p.M) / 8;
     // ---- stage the tile's records (coalesced 16-byte copies) and C_{rt-1}
     {
