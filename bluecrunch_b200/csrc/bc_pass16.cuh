@@ -122,12 +122,7 @@ template <int L> struct Pass16 {
 // registers.  No global twiddle loads remain on the unit's path.
 constexpr int TILE_TW = 18;  // tile factors per unit
 
-// T(m) = e^{-2 pi i m/(4M)} for |m| < 4M: sincospi of m/(2M).
-__device__ __forceinline__ double2 t4m(long long m, double twoM) {
-  double sn, cs;
-  sincospi((double)m / twoM, &sn, &cs);
-  return make_double2(cs, -sn);
-}
+// T(m) = e^{-2 pi i m/(4M)}: t4m(m, 2M) (bc_pipe.cuh).
 
 struct ColTw16 {
   double2 c0, cst, cb1;

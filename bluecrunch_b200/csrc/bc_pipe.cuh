@@ -43,7 +43,7 @@ template <int L> struct PassTile {
   // dynamic shared memory of k2_mid / k2_outer_inv: two tiles, the stage
   // twiddles, the outer pass's weights (outer_inv only), 1024 bytes of slack
   // for aligning the tiles
-  static constexpr size_t SMEM_MID = 2 * (size_t)BYTES + (size_t)TWN * 16 + 1024;
+  static constexpr size_t SMEM_MID = 2 * (size_t)BYTES + (size_t)TWN * 16 + 2 * (size_t)(L / PTS + 1) * 16 + 1024;
   static constexpr size_t SMEM_OUTER_INV = SMEM_MID + (size_t)L * 16;
 };
 
@@ -101,20 +101,46 @@ __device__ __forceinline__ void outer_twiddles(const Tw2 &T, int col, int t, dou
   else twiddle_run(T, (uint64_t)col * (4 * t - 1), false, (uint64_t)col * 4 * TC, w);
 }
 
+// e^{-2 pi i m/(2 h)} for |m| < 2h: sincospi of m/h.  With h = 2M it is the
+// outer passes' e^{-2 pi i m/(4M)}; with h = S1/2 the middle passes'
+// e^{-2 pi i m/(L2 Lr)}.
+__device__ __forceinline__ double2 t4m(long long m, double h) {
+  double sn, cs;
+  sincospi((double)m / h, &sn, &cs);
+  return make_double2(cs, -sn);
+}
+
 // ------------------------------------------------------------------ middle (3 levels)
 // Units: (item, operand, block k1, column tile).  Map: 4-d view of a slab,
 // (2*Lr doubles, L2 rows, L1 blocks, items).
+// Twiddles e^{-2 pi i col k2/(L2 Lr)} of a thread's points k2 = t + TC i,
+// col = tile W + s, as a base and a step with a running product; both are
+// products of a tile factor and a column factor (T(col x) = T(tile W x)
+// T(s x)): the TC + 1 tile factors T(tile W t) (t < TC) and T(tile W TC) are
+// computed once per unit by a few lanes of each warp (sincospi) into shared
+// memory, the column factors T(s t) and T(s TC) stay in registers.  No
+// global twiddle loads remain on the unit's path.
+template <int TC, int W, int NT>
+__device__ __forceinline__ void mid_tile_tw(double2 *fac, int tile, double h) {
+  constexpr int NF = TC + 1, NW = NT / 32, PER = (NF + NW - 1) / NW;
+  const int lane = threadIdx.x & 31, j = (threadIdx.x >> 5) * PER + lane;
+  if (lane < PER && j < NF) fac[j] = t4m((long long)tile * W * (j < TC ? j : TC), h);
+}
+
 template <int L, bool INV>
 __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
     k2_mid(ClassParams p, const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB) {
   using T = PassTile<L>;
-  constexpr int W = T::W, TC = L / PTS;
+  constexpr int W = T::W, TC = L / PTS, NT = T::NT;
   extern __shared__ unsigned char smraw[];
   __shared__ uint64_t bars[2];
   double2 *const buf0 = align1024(smraw);  // stage st's tile at buf0 + st * L * W
   double2 *twS = buf0 + 2 * L * W;
+  double2 *fac = twS + T::TWN;  // tile factors of unit parity st at fac + st * (TC + 1)
   table_to_smem(twS, p.twL2, T::TWN);
   const int tid = threadIdx.x, s = tid % W, t = tid / W;
+  const double h = 0.5 * (double)p.S1;
+  const double2 cb = t4m((long long)s * t, h), cs = t4m((long long)s * TC, h);
   // unit counts stay far below 2^32 (a class holds at most 2^33 points, 2048 per unit)
   const unsigned tiles = p.Lr / W;
   // forward: the A units of every item, then the B slab's slots (map mB's
@@ -137,11 +163,24 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
     fence_proxy_async_smem();
     tile_load_4d<L, W>(buf0 + st * L * W, op ? &mB : &mA, &bars[st], tile * W, blk, slot);
   };
+  auto tile_of = [&](unsigned u) -> int {
+    int item, op, slot, blk, tile;
+    decode(u, item, op, slot, blk, tile);
+    return tile;
+  };
+  // the unit's twiddles from its tile factors (fac) and the column factors
+  auto twiddles = [&](const double2 *f, double2 (&w)[PTS]) {
+    const double2 step = cmul(f[TC], cs);
+    w[0] = cmul(f[t], cb);
+#pragma unroll
+    for (int i = 1; i < PTS; i++) w[i] = cmul(w[i - 1], step);
+  };
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_mbar_init();
   }
+  if (blockIdx.x < total) mid_tile_tw<TC, W, NT>(fac, tile_of(blockIdx.x), h);
   __syncthreads();
   unsigned phases = 0;  // bit st: parity to wait for on bars[st]
   int st = 0;
@@ -156,9 +195,7 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
     double2 *g = (op ? it.bufB : it.bufA) + (unsigned)blk * (unsigned)p.S1;
     const int col = tile * W + s;
     double2 v[PTS], w[PTS];
-    // e^{-2 pi i col k2/(L2 Lr)} = table index 4 L1 col k2 of the 4M table
-    // (global loads issued before the wait so their latency overlaps it)
-    twiddle_run(p.tw4M, (uint64_t)4 * p.L1 * col * t, false, (uint64_t)4 * p.L1 * col * TC, w);
+    if (INV) twiddles(fac + st * (TC + 1), w);
     const unsigned par = (phases >> st) & 1u;
     const bool ok = mbar_wait(&bars[st], par);
     phases ^= 1u << st;
@@ -178,7 +215,11 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
       }
       return;
     }
+    // the next unit's tile factors (its parity's slot was last read before
+    // the barrier above)
+    if (un < total) mid_tile_tw<TC, W, NT>(fac + (st ^ 1) * (TC + 1), tile_of(un), h);
     block_fft<L, W, INV>(v, t, s, bf, twS);
+    if (!INV) twiddles(fac + st * (TC + 1), w);
 #pragma unroll
     for (int i = 0; i < PTS; i++) {
       const unsigned k2 = t + i * TC;
