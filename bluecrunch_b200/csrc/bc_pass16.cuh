@@ -312,6 +312,10 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
     fence_mbar_init();
   }
   __syncthreads();
+  // largest rounding error of this thread's units of the current item,
+  // published (one atomic per warp) when the item changes and at the end
+  double err_acc = 0.0;
+  int err_item = -1;
   unsigned phases = 0;  // bit st: parity to wait for on bars[st]
   int st = 0;
   unsigned u = blockIdx.x;
@@ -328,6 +332,11 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
       tile_load_3d<L, W>(buf0 + (st ^ 1) * L * W, &mA, &bars[st ^ 1], (int)(un - qn * tiles) * W, (int)qn);
     }
     const int item = (int)fd_tiles.div(u), tile = (int)(u - (unsigned)item * tiles);
+    if (item != err_item) {  // uniform over the CTA: every thread is on unit u
+      if (err_item >= 0) atomic_max_err(p.items[err_item].err, err_acc);
+      err_acc = 0.0;
+      err_item = item;
+    }
     const ItemDesc &it = p.items[item];
     const unsigned par = (phases >> st) & 1u;
     const bool ok = mbar_wait(&bars[st], par);
@@ -355,16 +364,14 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
     // the next unit's tile factors (read after this unit's last barrier)
     if (un < total) tile_tw16<R, W, NT>(fac + (st ^ 1) * TILE_TW, (int)(un % tiles), twoM);
     block16<L, W, true>(v, t, s, bf, twS);
-    double err = 0.0;
 #pragma unroll
     for (int i = 0; i < P16; i++) {
       const int n1 = t + i * R;
       double2 z = cmul(v[i], pwS[n1]);
       double re = rint(z.x), im = rint(z.y);
-      err = fmax(err, round_check(z, re, im));
+      err_acc = fmax(err_acc, round_check(z, re, im));
       bf[bidx<L>(n1, s)] = make_double2(re, im);
     }
-    atomic_max_err(it.err, err);
     __syncthreads();
     // run records: one 8-column group of one row per (thread, q); L*G rows x
     // groups over NT threads
@@ -386,6 +393,7 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
     __syncthreads();  // the tile buffer is reloaded next iteration
     st ^= 1;
   }
+  if (err_item >= 0) atomic_max_err(p.items[err_item].err, err_acc);
 }
 
 }  // namespace bc
