@@ -1655,6 +1655,17 @@ int radix_tree_core(const uint32_t *dy, size_t ylen, const bc_radix_node *nodes,
     prod_off[i] = prod_total;
     prod_total += (std::max(prod_len[i], x.n) + 63) & ~size_t(63);
   }
+  // $BC_STATS: time of each step (products per depth, leaves, merges) on stderr
+  const bool stats = getenv("BC_STATS") != nullptr;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto secs = [](std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  };
+  auto sync_secs = [&](std::chrono::steady_clock::time_point t0) -> double {
+    if (stats) cudaStreamSynchronize(g.stream);
+    return secs(t0);
+  };
+  double t_mul_total = 0;
   // device buffers: products, digits
   DevBuf dprod, ds, dmeta;
   int r;
@@ -1675,9 +1686,17 @@ int radix_tree_core(const uint32_t *dy, size_t ylen, const bc_radix_node *nodes,
       yptr[x.child_l] = C + (x.n - nodes[x.child_l].n);
     }
     bc_batch_stats st{};
+    const auto t0 = now();
     if (!md.empty() && (r = mul_batch_locked(md.data(), md.size(), &st, nullptr, BC_BATCH_DEVICE_OPERANDS)))
       return r;
+    if (stats) {
+      const double t = secs(t0);
+      t_mul_total += t;
+      fprintf(stderr, "      conversion depth %d: %zu products, %.4f s (device %.4f s)\n", d, md.size(), t,
+              st.device_ms / 1e3);
+    }
   }
+  auto t_step = now();
   // leaves
   std::vector<RadixLeaf> lv;
   for (size_t i = 0; i < nn; i++) {
@@ -1689,6 +1708,8 @@ int radix_tree_core(const uint32_t *dy, size_t ylen, const bc_radix_node *nodes,
     lv.push_back({yptr[i], dsd + s_off[i], (uint32_t)ylenv[i], (uint32_t)x.n, (uint32_t)x.k, 0u});
   }
   if ((r = radix_leaves_device(lv, alpha))) return r;
+  const double t_leaves = sync_secs(t_step);
+  t_step = now();
   // bottom-up merges, one depth at a time
   const size_t o_flag = align256(nn * sizeof(MergeDesc));
   if ((r = dmeta.alloc(o_flag + nn * 4))) return r;
@@ -1715,6 +1736,9 @@ int radix_tree_core(const uint32_t *dy, size_t ylen, const bc_radix_node *nodes,
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(g.stream));  // mg is rewritten for the next depth
   }
+  if (stats)
+    fprintf(stderr, "      conversion tree: products %.3f s, %zu leaves %.3f s, merges %.3f s\n", t_mul_total, lv.size(),
+            t_leaves, sync_secs(t_step));
   // the root's digits: to the caller's device array, or through the ring
   if (is_device_ptr(out)) {
     CK(cudaMemcpyAsync(out, dsd + s_off[0], nodes[0].k * 4, cudaMemcpyDeviceToDevice, g.stream));
@@ -1815,6 +1839,7 @@ int radix_tree_pow_locked(const uint32_t *y, size_t ylen, const bc_radix_node *n
   tlen[0] = t0len;
   dtab[0] = (const uint32_t *)tab[0].p;
   bc_batch_stats st{};
+  const auto t_tab = std::chrono::steady_clock::now();
   for (int i = 1; i < ntable; i++) {
     const int j = steps[i].src, op = steps[i].op;
     const uint32_t *X = dtab[j];
@@ -1845,6 +1870,11 @@ int radix_tree_pow_locked(const uint32_t *y, size_t ylen, const bc_radix_node *n
       }
     }
     dtab[i] = (const uint32_t *)tab[i].p;
+  }
+  if (getenv("BC_STATS")) {
+    cudaStreamSynchronize(g.stream);
+    fprintf(stderr, "      conversion power table: %d entries, %.3f s\n", ntable,
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t_tab).count());
   }
   return radix_tree_core(dy, ylen, nodes, nn, dtab.data(), tlen.data(), ntable, alpha, out);
 }

@@ -11,10 +11,16 @@
 // window's top limb is zero; the carry out of the window is dropped; the
 // digit is limb n after the multiply and lands in s[k - i].
 //
-// One warp per leaf: lane l holds limbs [l*RS, (l+1)*RS) in registers, each
-// lane multiplies its limbs with a local carry chain, and the carry out of a
-// lane enters the next lane (a carry of that carry past a full lane is
-// astronomically rare and handled by a bounded ripple).
+// One warp per leaf, RS limbs per lane in registers, laid out so that limb n
+// is the last limb of lane 31 (lane l holds limbs base + l*RS ... base +
+// (l+1)*RS - 1, base = n + 1 - 32*RS): the digit is then one fixed register,
+// and the window's top limb, which enters each round after the first as
+// zero, is that same register.  Limbs above n are not held: carries only move
+// up, so they never reach limb n (in the first round the window reaches limb
+// len >= n, but what it computes above n is dropped with the carry out).
+// Each lane multiplies its limbs with a local carry chain; the carry out of a
+// lane enters the next lane's lowest limb, and a carry out of that limb
+// (astronomically rare) ripples further by a bounded loop.
 #pragma once
 #include <cstdint>
 
@@ -44,64 +50,64 @@ __global__ void __launch_bounds__(32 * RADIX_WARPS) k_radix_leaves(const RadixLe
       if (lane == 0) atomicOr(flags, 1u);
       continue;
     }
-    // coalesced load into shared memory (one pad word per 32), then each
-    // lane takes its RS consecutive limbs
-    for (uint32_t j = lane; j < (uint32_t)RADIX_WINDOW; j += 32) sm[j + (j >> 5)] = j < lf.len ? lf.y[j] : 0u;
+    // limb j sits at index j - base (base = n + 1 - RADIX_WINDOW <= 0): a
+    // coalesced load into shared memory (one pad word per 32), then each lane
+    // takes its RS consecutive indices
+    const int base = (int)lf.n + 1 - RADIX_WINDOW;
+    for (int t = lane; t < RADIX_WINDOW; t += 32) {
+      const int j = t + base;
+      sm[t + (t >> 5)] = (j >= 0 && j < (int)lf.len) ? lf.y[j] : 0u;
+    }
     __syncwarp();
     uint32_t x[RS];
 #pragma unroll
     for (int q = 0; q < RS; q++) {
-      const int j = lane * RS + q;
-      x[q] = sm[j + (j >> 5)];
+      const int t = lane * RS + q;
+      x[q] = sm[t + (t >> 5)];
     }
     __syncwarp();
-    const uint32_t j0 = (uint32_t)lane * RS;  // this lane's first limb
-    const uint32_t owner = lf.n / RS, slot = lf.n % RS;
+    const int j0 = lane * RS + base;  // limb of x[0]
     for (uint32_t i = 1; i <= lf.k; i++) {
-      const uint32_t lo = i == 1 ? 0u : (uint32_t)floor(alpha * (double)(i - 1));
-      const uint32_t hi = i == 1 ? L : lf.n + 1;
-      // multiply the window by 10^9 (its top limb enters as zero)
+      const int lo = i == 1 ? 0 : (int)floor(alpha * (double)(i - 1));
+      // rounds after the first: the window's top limb (limb n, the last
+      // digit) enters as zero
+      if (i > 1 && lane == 31) x[RS - 1] = 0;
+      // multiply the window [lo, n] by 10^9
       uint32_t c = 0;
 #pragma unroll
       for (int q = 0; q < RS; q++) {
-        const uint32_t j = j0 + q;
-        if (j >= lo && j < hi) {
-          const uint32_t xin = j == hi - 1 ? 0u : x[q];
-          const unsigned long long v = (unsigned long long)xin * DEC_BASE + c;
+        if (j0 + q >= lo) {
+          const unsigned long long v = (unsigned long long)x[q] * DEC_BASE + c;
           x[q] = (uint32_t)v;
           c = (uint32_t)(v >> 32);
         }
       }
-      // the window's top lane drops its carry; the others pass it up
-      const bool top_lane = hi - 1 >= j0 && hi - 1 < j0 + RS;
-      const bool above = j0 >= hi;
-      uint32_t out = (top_lane || above) ? 0u : c;
-      uint32_t cin = __shfl_up_sync(~0u, out, 1);
+      // the carry out of lane l enters lane l+1 at its lowest limb, which is
+      // inside the window whenever the carry is nonzero; lane 31's is dropped
+      uint32_t cin = __shfl_up_sync(~0u, c, 1);
       if (lane == 0) cin = 0;
-      // add the carry in at the lane's lowest window limb; a carry out of the
-      // lane ripples to the next lane (bounded: at most 32 rounds)
-      for (int round = 0; round < 32; round++) {
-        uint32_t t = cin;
+      {
+        const unsigned long long v = (unsigned long long)x[0] + cin;
+        x[0] = (uint32_t)v;
+        uint32_t t = (uint32_t)(v >> 32);
+        // rare: the lowest limb overflowed; ripple through the lane and on
+        // into the next lanes (bounded: at most 32 rounds)
+        for (int round = 0; round < 32 && __any_sync(~0u, t != 0); round++) {
 #pragma unroll
-        for (int q = 0; q < RS; q++) {
-          const uint32_t j = j0 + q;
-          if (t && j >= lo && j < hi) {
-            const unsigned long long v = (unsigned long long)x[q] + t;
-            x[q] = (uint32_t)v;
-            t = (uint32_t)(v >> 32);
+          for (int q = 1; q < RS; q++) {
+            const unsigned long long w = (unsigned long long)x[q] + t;
+            x[q] = (uint32_t)w;
+            t = (uint32_t)(w >> 32);
           }
+          uint32_t up = __shfl_up_sync(~0u, t, 1);
+          if (lane == 0) up = 0;
+          const unsigned long long w = (unsigned long long)x[0] + up;
+          x[0] = (uint32_t)w;
+          t = (uint32_t)(w >> 32);
         }
-        const uint32_t ov = (top_lane || above) ? 0u : t;
-        if (!__any_sync(~0u, ov != 0)) break;
-        cin = __shfl_up_sync(~0u, ov, 1);
-        if (lane == 0) cin = 0;
       }
-      // the digit: limb n
-      uint32_t dgt = 0;
-#pragma unroll
-      for (int q = 0; q < RS; q++) dgt = (uint32_t)q == slot ? x[q] : dgt;
-      dgt = __shfl_sync(~0u, dgt, (int)owner);
-      if (lane == 0) lf.s[lf.k - i] = dgt;
+      // the digit: limb n, the last register of lane 31
+      if (lane == 31) lf.s[lf.k - i] = x[RS - 1];
     }
   }
 }
