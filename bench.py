@@ -401,6 +401,22 @@ def run_batched(bc, torch, stream, n=8192, sibling=False, per_call=True, reps=2)
            "launches_per_batch": st["launches"], "batched_ms": round(batched_ms, 3),
            "batched_GBps": round(nbytes / (batched_ms * 1e-3) / 1e9, 1),
            "products_per_s": round(n / (batched_ms * 1e-3), 1), "modcheck_sample_ok": bool(ok)}
+    # the same batch as one CUDA graph launch (BC_BATCH_GRAPH): the first call
+    # instantiates, the timed ones update the kept executable graph in place
+    out.zero_()
+    bc.mul_batch_desc(descs, n, bc.BATCH_GRAPH)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        sg = bc.mul_batch_desc(descs, n, bc.BATCH_GRAPH)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    graph_ms = e0.elapsed_time(e1) / reps
+    out_g = out.cpu().numpy().view(np.uint32)
+    gok = bool(np.array_equal(out_g, out_h))
+    res.update({"graph_ms": round(graph_ms, 3), "graph_launches_per_batch": sg["graph_launches"],
+                "graph_kernel_nodes": sg["graph_nodes"], "graph_updated_in_place": sg["graph_updates"] == 1,
+                "graph_GBps": round(nbytes / (graph_ms * 1e-3) / 1e9, 1), "graph_equals_batched": gok})
     if per_call:
         out.zero_()
         lib = bc._lib()

@@ -59,7 +59,11 @@ class MulDesc(ctypes.Structure):
 class BatchStats(ctypes.Structure):
     _fields_ = [("items", _sz), ("classes", _sz), ("launches", _sz), ("retries", ctypes.c_int),
                 ("max_round_err", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("total_ms", ctypes.c_double), ("h2d_bytes", _sz), ("d2h_bytes", _sz)]
+                ("total_ms", ctypes.c_double), ("h2d_bytes", _sz), ("d2h_bytes", _sz),
+                ("graph_launches", _sz), ("graph_nodes", _sz), ("graph_updates", _sz)]
+
+
+BATCH_HOST_OPERANDS, BATCH_DEVICE_OPERANDS, BATCH_GRAPH = 1, 2, 4
 
 
 class PlanInfo(ctypes.Structure):
@@ -233,10 +237,14 @@ def decimal_write(limbs, top, n, maxbytes, fd, offset=0):
     del keep
 
 
-def mul_batch_desc(descs, n):
-    """Raw batch call on a prepared (MulDesc * n) array; returns stats dict."""
+def mul_batch_desc(descs, n, flags=0):
+    """Raw batch call on a prepared (MulDesc * n) array (bc_gpu_mul_batch, or
+    bc_gpu_mul_batch_flags with `flags`, e.g. BATCH_GRAPH); returns stats dict."""
     st = BatchStats()
-    _check(_lib().bc_gpu_mul_batch(descs, n, ctypes.byref(st)), "bc_gpu_mul_batch")
+    if flags:
+        _check(_lib().bc_gpu_mul_batch_flags(descs, n, flags, ctypes.byref(st)), "bc_gpu_mul_batch_flags")
+    else:
+        _check(_lib().bc_gpu_mul_batch(descs, n, ctypes.byref(st)), "bc_gpu_mul_batch")
     return {k: getattr(st, k) for k, _ in BatchStats._fields_}
 
 

@@ -150,6 +150,11 @@ struct Ctx {
   // data): a small class's kernels fill the SMs a large one leaves idle
   cudaStream_t class_stream[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t class_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // [4]: fork
+  // BC_BATCH_GRAPH: the launches are captured on cap_stream (which never runs
+  // work itself) and the kept executable graph is updated or re-instantiated
+  bool graph_all = false;  // $BC_GRAPH=1: every batch as a graph
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
   std::vector<std::pair<const char *, double>> ktimes;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;
@@ -1075,9 +1080,51 @@ int pin_small_reserve(size_t bytes) {
   return BC_OK;
 }
 
+// Ends a stream capture that an error path leaves open, so that the capture
+// stream is usable by the next call.
+struct CaptureGuard {
+  cudaStream_t s = nullptr;
+  ~CaptureGuard() {
+    if (!s) return;
+    cudaGraph_t gr = nullptr;
+    cudaStreamEndCapture(s, &gr);
+    if (gr) cudaGraphDestroy(gr);
+    cudaGetLastError();
+  }
+};
+
+// The captured graph replaces the kept executable graph's contents when its
+// launch structure is the same (cudaGraphExecUpdate), else it is instantiated
+// anew; then one cudaGraphLaunch on the library stream runs every class.
+int launch_graph(cudaGraph_t gr, bc_batch_stats *st) {
+  size_t nodes = 0;
+  cudaGraphGetNodes(gr, nullptr, &nodes);
+  bool updated = false;
+  if (g.gexec) {
+    cudaGraphExecUpdateResultInfo info;
+    updated = cudaGraphExecUpdate(g.gexec, gr, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();  // a structural mismatch is not an error: instantiate
+      cudaGraphExecDestroy(g.gexec);
+      g.gexec = nullptr;
+    }
+  }
+  cudaError_t e = updated ? cudaSuccess : cudaGraphInstantiate(&g.gexec, gr, 0);
+  if (e != cudaSuccess) g.gexec = nullptr;
+  cudaGraphDestroy(gr);
+  CK(e);
+  CK(cudaEventRecord(g.ev0, g.stream));
+  CK(cudaGraphLaunch(g.gexec, g.stream));
+  st->graph_launches++;
+  st->graph_nodes += nodes;
+  st->graph_updates += updated ? 1 : 0;
+  return BC_OK;
+}
+
 int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_stats *st, unsigned flags_in) {
   const bool all_host = flags_in & BC_BATCH_HOST_OPERANDS;
   const bool all_dev = flags_in & BC_BATCH_DEVICE_OPERANDS;
+  const bool graph = ((flags_in & BC_BATCH_GRAPH) || g.graph_all) && !g.time_kernels && !g.fused;
   const size_t nw = works.size();
   PhaseTimer pt(&g_prof.layout);
   g_prof.items += nw;
@@ -1234,7 +1281,7 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     else if (pin_inB_off[i] != SIZE_MAX) runs[i].dB = (const uint32_t *)(base + off_stage_in + pin_inB_off[i]);
     else {
       runs[i].dB = (const uint32_t *)(base + slots[i].off_dB);
-      if (nw == 1 && pl.shape.levels >= 2 && pl.BL >= ((size_t)1 << 20)) {
+      if (nw == 1 && pl.shape.levels >= 2 && pl.BL >= ((size_t)1 << 20) && !graph) {
         // a single large product: B crosses on the copy stream (after the
         // library stream's earlier work, which may still read this slot)
         // while the outer pass packs A
@@ -1320,13 +1367,27 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   // joined back into the library stream).  Per-kernel timing and the
   // cooperative fused kernel keep the single stream.
   pt.next(&g_prof.launch);
-  CK(cudaEventRecord(g.ev0, g.stream));
+  // graph mode: every table exists before the capture (a new table's upload
+  // synchronises the library stream), launches go to the capture stream
+  cudaStream_t lstream = g.stream;
+  CaptureGuard cap;
+  if (graph) {
+    for (auto &c : classes) {
+      Tables *tb = nullptr;
+      if ((r = ensure_tables(works[c.second[0]]->pl.shape, &tb))) return r;
+    }
+    if (!g.cap_stream) CK(cudaStreamCreateWithFlags(&g.cap_stream, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(g.cap_stream, cudaStreamCaptureModeRelaxed));
+    cap.s = lstream = g.cap_stream;
+  } else {
+    CK(cudaEventRecord(g.ev0, g.stream));
+  }
   const int nstreams = (classes.size() > 1 && !g.time_kernels && !g.fused && !b_late)
                            ? (int)std::min<size_t>(classes.size(), 4) : 0;
   if (nstreams) {
     for (int k = 0; k < 5; k++)
       if (!g.class_ev[k]) CK(cudaEventCreateWithFlags(&g.class_ev[k], cudaEventDisableTiming));
-    CK(cudaEventRecord(g.class_ev[4], g.stream));
+    CK(cudaEventRecord(g.class_ev[4], lstream));
     for (int k = 0; k < nstreams; k++) {
       if (!g.class_stream[k]) CK(cudaStreamCreateWithFlags(&g.class_stream[k], cudaStreamNonBlocking));
       CK(cudaStreamWaitEvent(g.class_stream[k], g.class_ev[4], 0));
@@ -1362,7 +1423,7 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     }
     p.carry_tiles = tiles;
     const ClassSlab &cs = slab[c.first];
-    cudaStream_t cstream = nstreams ? g.class_stream[cls % nstreams] : g.stream;
+    cudaStream_t cstream = nstreams ? g.class_stream[cls % nstreams] : lstream;
     if ((r = launch_class(s, sq, p, (long long)n, tiles, (double2 *)(base + cs.offA),
                           sq ? nullptr : (double2 *)(base + cs.offB), cstream, true, &st->launches,
                           b_late ? g.copy_ev[1] : nullptr, w16)))
@@ -1372,7 +1433,13 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
   }
   for (int k = 0; k < nstreams; k++) {
     CK(cudaEventRecord(g.class_ev[k], g.class_stream[k]));
-    CK(cudaStreamWaitEvent(g.stream, g.class_ev[k], 0));
+    CK(cudaStreamWaitEvent(lstream, g.class_ev[k], 0));
+  }
+  if (graph) {
+    cudaGraph_t gr = nullptr;
+    cap.s = nullptr;
+    CK(cudaStreamEndCapture(g.cap_stream, &gr));
+    if ((r = launch_graph(gr, st))) return r;
   }
   CK(cudaEventRecord(g.ev1, g.stream));
   st->classes += classes.size();
@@ -2533,6 +2600,8 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
     g.fused = fu && fu[0] == '1';
     const char *sb = getenv("BC_SHARE_B");
     g.share_b = !(sb && sb[0] == '0');
+    const char *gr = getenv("BC_GRAPH");
+    g.graph_all = gr && gr[0] == '1';
   }
   load_width_file(c.tune_path);
   {
@@ -2575,6 +2644,8 @@ int bc_gpu_shutdown(void) {
   if (g.ev1) cudaEventDestroy(g.ev1);
   if (g.own_stream) cudaStreamDestroy(g.own_stream);
   if (g.copy_stream) cudaStreamDestroy(g.copy_stream);
+  if (g.gexec) cudaGraphExecDestroy(g.gexec);
+  if (g.cap_stream) cudaStreamDestroy(g.cap_stream);
   for (auto &cs : g.class_stream)
     if (cs) cudaStreamDestroy(cs);
   for (auto &e : g.class_ev)

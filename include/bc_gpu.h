@@ -74,6 +74,9 @@ typedef struct {
   double device_ms;       /* GPU time of the kernels */
   double total_ms;        /* wall time including copies */
   size_t h2d_bytes, d2h_bytes;
+  size_t graph_launches;  /* CUDA graph launches (BC_BATCH_GRAPH; per attempt) */
+  size_t graph_nodes;     /* kernel and event nodes in those graphs */
+  size_t graph_updates;   /* of them, the kept executable graph updated in place */
 } bc_batch_stats;
 
 /* Plan of one product (no GPU needed; for inspection and tests). */
@@ -112,7 +115,18 @@ int bc_gpu_mul_small_batch(const bc_mul_desc *items, size_t n);
  * host memory, BC_BATCH_DEVICE_OPERANDS every one to be device memory (each
  * skips the per-pointer memory query, which dominates batches of millions of
  * small products). */
-enum { BC_BATCH_HOST_OPERANDS = 1, BC_BATCH_DEVICE_OPERANDS = 2 };
+enum { BC_BATCH_HOST_OPERANDS = 1, BC_BATCH_DEVICE_OPERANDS = 2, BC_BATCH_GRAPH = 4 };
+/* BC_BATCH_GRAPH (or $BC_GRAPH=1 for every batch): the batch's passes, every
+ * length bucket on its class stream, are captured into one CUDA graph and
+ * started with a single cudaGraphLaunch.  The library keeps the executable
+ * graph and updates it in place (cudaGraphExecUpdate) when the next batch has
+ * the same launch structure, so a batch of the same lengths repeated (one
+ * tree level after another of the same shape, a benchmark loop) pays neither
+ * per-kernel launch calls nor a new instantiation.  Products, rounding checks
+ * and retries are the same as without the flag; per-kernel timing
+ * (bc_gpu_time_kernels) and the opt-in fused middle pass ($BC_FUSED=1) turn
+ * it off.  The reference has no counterpart (its task tree, main.c:82-90,
+ * runs products one call each). */
 int bc_gpu_mul_batch_flags(const bc_mul_desc *items, size_t n, unsigned flags, bc_batch_stats *stats);
 
 /* The binary-splitting sum of e's series on the GPU: P and Q with
