@@ -149,3 +149,31 @@ def test_shape_candidates_and_table():
         assert lib.bc_gpu_check_shapes() == 0
         for M in bc.lengths():
             bc.set_shape(M)
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """The Python mirrors of bc_batch_stats, bc_mul_stats, bc_mul_desc and
+    bc_plan_info have the C compiler's size and field offsets, and the batch
+    flags have the header's values."""
+    import subprocess
+    structs = {"bc_batch_stats": bc.BatchStats, "bc_mul_stats": bc.MulStats, "bc_mul_desc": bc.MulDesc,
+               "bc_plan_info": bc.PlanInfo}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bc_gpu.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in py._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines.append('printf("flags %d %d %d\\n", BC_BATCH_HOST_OPERANDS, BC_BATCH_DEVICE_OPERANDS, BC_BATCH_GRAPH);')
+    lines.append("return 0; }")
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.check_call(["gcc", "-std=c11", "-I" + os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
+    got = {}
+    for ln in subprocess.check_output([str(exe)], text=True).splitlines():
+        k, v = ln.rsplit(" ", 1) if not ln.startswith("flags") else (ln[:5], ln[6:])
+        got[k] = v
+    for cname, py in structs.items():
+        assert int(got[cname + " sizeof"]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got["%s %s" % (cname, f)]) == getattr(py, f).offset, (cname, f)
+    assert got["flags"].split() == [str(bc.BATCH_HOST_OPERANDS), str(bc.BATCH_DEVICE_OPERANDS), str(bc.BATCH_GRAPH)]
