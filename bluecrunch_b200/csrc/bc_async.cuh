@@ -100,6 +100,16 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_b
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// ------------------------------------------------------------------ programmatic dependent launch
+// A pass launched with programmatic stream serialisation may start while the
+// previous pass of its stream is still finishing: its CTAs set up shared
+// memory from read-only tables, then pdl_wait() blocks until the previous
+// grid has completed and its writes are visible (a no-op for a normal
+// launch).  Every global access to data another pass reads or writes comes
+// after it.  pdl_trigger() lets the next pass of the stream be launched.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");

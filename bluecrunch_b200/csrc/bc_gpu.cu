@@ -153,6 +153,9 @@ struct Ctx {
   // BC_BATCH_GRAPH: the launches are captured on cap_stream (which never runs
   // work itself) and the kept executable graph is updated or re-instantiated
   bool graph_all = false;  // $BC_GRAPH=1: every batch as a graph
+  // passes after a class's first one start while the previous pass drains
+  // (programmatic dependent launch; $BC_PDL=0: plain stream order)
+  bool pdl = true;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<std::pair<const char *, double>> ktimes;
@@ -593,8 +596,11 @@ int prepare(const KInfo &k, int *grid_cap) {
   return BC_OK;
 }
 
+// pdl: launch with programmatic stream serialisation (the kernel may start
+// while the previous kernel of the stream finishes; it waits in pdl_wait
+// before touching data that kernel reads or writes)
 int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunch, cudaStream_t stream, bool timed,
-           const CUtensorMap *mA = nullptr, const CUtensorMap *mB = nullptr) {
+           const CUtensorMap *mA = nullptr, const CUtensorMap *mB = nullptr, bool pdl = false) {
   int cap = 0;
   int r = prepare(k, &cap);
   if (r) return r;
@@ -605,8 +611,23 @@ int launch(const KInfo &k, long long units, const ClassParams &p, size_t *nlaunc
   if (mB) b = *mB;
   else b = a;
   void *args[3] = {&pc, &a, &b};
-  if (k.coop) CK(cudaLaunchCooperativeKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
-  else CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
+  if (k.coop) {
+    CK(cudaLaunchCooperativeKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
+  } else if (pdl) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(k.threads);
+    cfg.dynamicSmemBytes = k.smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelExC(&cfg, k.fn, args));
+  } else {
+    CK(cudaLaunchKernel(k.fn, dim3(grid), dim3(k.threads), args, k.smem, stream));
+  }
   (*nlaunch)++;
   if (timed && g.time_kernels) {
     cudaEvent_t e;
@@ -710,8 +731,11 @@ KInfo get_fused(int L2, bool sq) {
 // counter and status words zeroed by the caller.
 int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, unsigned long long carry_tiles,
                  double2 *slabA, double2 *slabB, cudaStream_t stream, bool timed, size_t *nl,
-                 cudaEvent_t b_ready = nullptr, bool w16 = false) {
+                 cudaEvent_t b_ready = nullptr, bool w16 = false, bool pdl_ok = false) {
   int r;
+  // the first pass follows copies or event waits: a normal launch; every
+  // later pass of the class follows the previous pass directly
+  bool pdl = false;
   if (!shape_launch_ok(s, sq)) return fail(BC_ERR_INVALID);
   if (s.levels == 1) return launch(get_small(s.M, sq), n, p, nl, stream, timed);
   const cuuint64_t M16 = (cuuint64_t)s.M * 16, S1 = (cuuint64_t)p.S1, Lr = (cuuint64_t)p.Lr;
@@ -731,6 +755,7 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
   } else if ((r = launch(ko, (n + nb) * (long long)(S1 / W1), p, nl, stream, timed))) {
     return r;
   }
+  pdl = pdl_ok;
   if (fused_ok(s) && p.blkdone && (sq || p.nb == n)) {
     // the middle (column pass, row products, inverse column pass) in one
     // persistent cooperative kernel; per-block counters in p.blkdone
@@ -759,7 +784,8 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
       if ((r = encode_map(&midA, slabA, 4, dims, str, box))) return r;
       const cuuint64_t dimsB[4] = {dims[0], dims[1], dims[2], (cuuint64_t)std::max<long long>(nb, 1)};
       if (!sq && (r = encode_map(&midB, slabB, 4, dimsB, str, box))) return r;
-      if ((r = launch(km, (n + nb) * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB)))
+      if ((r = launch(km, (n + nb) * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, sq ? &midA : &midB,
+                      pdl)))
         return r;
     }
     if (get_rows(s.Lr, sq).warp_rows) {
@@ -767,7 +793,7 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
       KInfo kr = get_rows(s.Lr, sq);
       const long long rows = n * (long long)(s.M / s.Lr);
       const long long wpc = kr.threads / 32;  // rows (warps) per CTA
-      if ((r = launch(kr, (rows + wpc - 1) / wpc, p, nl, stream, timed))) return r;
+      if ((r = launch(kr, (rows + wpc - 1) / wpc, p, nl, stream, timed, nullptr, nullptr, pdl))) return r;
     } else {
       KInfo kr = get_rows(s.Lr, sq);
       const int NR = kr.threads / (s.Lr / PTS);
@@ -783,12 +809,12 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
       // B's rows by slot: nb slots of M/Lr rows
       const cuuint64_t dimsB[3] = {16, Lr / 8, (cuuint64_t)std::max<long long>(nb, 1) * (cuuint64_t)(s.M / s.Lr)};
       if (!sq && (r = encode_map(&rB, slabB, 3, dimsB, str, box))) return r;
-      if ((r = launch(kr, (long long)(rows / NR), p, nl, stream, timed, &rA, sq ? &rA : &rB))) return r;
+      if ((r = launch(kr, (long long)(rows / NR), p, nl, stream, timed, &rA, sq ? &rA : &rB, pdl))) return r;
     }
     if (s.levels == 3) {
       KInfo km = get_mid(s.L2, true);
       const int W2 = km.threads / (s.L2 / km.pts);
-      if ((r = launch(km, n * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, &midA))) return r;
+      if ((r = launch(km, n * s.L1 * (long long)(Lr / W2), p, nl, stream, timed, &midA, &midA, pdl))) return r;
     }
   }
   {
@@ -799,10 +825,10 @@ int launch_class(const Shape &s, bool sq, const ClassParams &p, long long n, uns
       return fail(BC_ERR_INVALID);
     CUtensorMap oA;
     if ((r = encode_map(&oA, slabA, 3, dims, str, box))) return r;
-    if ((r = launch(ki, n * (long long)(S1 / W1), p, nl, stream, timed, &oA))) return r;
+    if ((r = launch(ki, n * (long long)(S1 / W1), p, nl, stream, timed, &oA, nullptr, pdl))) return r;
   }
   KInfo kc{w16 ? (const void *)k_carry<128> : (const void *)k_carry<0>, CARRY_NT, 0, "carry", SIG_P};
-  return launch(kc, (long long)carry_tiles, p, nl, stream, timed);
+  return launch(kc, (long long)carry_tiles, p, nl, stream, timed, nullptr, nullptr, pdl);
 }
 
 ClassParams class_params(const Shape &s, const Tables &tb) {
@@ -1079,6 +1105,12 @@ int pin_small_reserve(size_t bytes) {
   g.pin_small_cap = want;
   return BC_OK;
 }
+
+// Longest transform whose passes use programmatic dependent launch.  On B200
+// it shortened every product up to 2^25 points (2^14-limb products by 14 %,
+// 2^20 by 5 %, 2^24 by 1 %) and left 2^27 unchanged, while the 2^28-point
+// products ran 2-3 % slower; above this length passes launch in plain order.
+constexpr size_t kPdlMaxPoints = size_t(1) << 27;
 
 // Ends a stream capture that an error path leaves open, so that the capture
 // stream is usable by the next call.
@@ -1426,7 +1458,8 @@ int run_attempt(const bc_mul_desc *items, std::vector<Work *> &works, bc_batch_s
     cudaStream_t cstream = nstreams ? g.class_stream[cls % nstreams] : lstream;
     if ((r = launch_class(s, sq, p, (long long)n, tiles, (double2 *)(base + cs.offA),
                           sq ? nullptr : (double2 *)(base + cs.offB), cstream, true, &st->launches,
-                          b_late ? g.copy_ev[1] : nullptr, w16)))
+                          b_late ? g.copy_ev[1] : nullptr, w16,
+                          g.pdl && !graph && !g.time_kernels && !g.fused && (size_t)s.M <= kPdlMaxPoints)))
       return r;
     first += n;
     cls++;
@@ -2602,6 +2635,8 @@ int bc_gpu_init(const bc_gpu_config *cfg) {
     g.share_b = !(sb && sb[0] == '0');
     const char *gr = getenv("BC_GRAPH");
     g.graph_all = gr && gr[0] == '1';
+    const char *pd = getenv("BC_PDL");
+    g.pdl = !(pd && pd[0] == '0');
   }
   load_width_file(c.tune_path);
   {

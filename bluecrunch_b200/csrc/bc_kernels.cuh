@@ -292,6 +292,8 @@ __global__ void __launch_bounds__(CARRY_NT) k_carry(ClassParams p) {
   __shared__ int s_delta;
   __shared__ long long s_cprev;
   const int tid = threadIdx.x;
+  pdl_wait();
+  pdl_trigger();
   for (;;) {
     if (tid == 0) s_unit = atomicAdd(p.counter, 1u);
     __syncthreads();

@@ -166,6 +166,7 @@ __device__ __forceinline__ OuterRun16 outer_run16(const double2 *fac, const ColT
 // cut, and land while this unit is transformed and stored.
 template <int L>
 __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB) k3_outer_fwd(ClassParams p) {
+  pdl_trigger();  // the first pass of a class: launched normally, lets the next one start early
   using T = Pass16<L>;
   using K = PackTile<L>;
   constexpr int W = T::W, R = T::R, NT = T::NT;
@@ -312,6 +313,8 @@ __global__ void __launch_bounds__(Pass16<L>::NT, Pass16<L>::MINB)
     fence_mbar_init();
   }
   __syncthreads();
+  pdl_wait();
+  pdl_trigger();
   // largest rounding error of this thread's units of the current item,
   // published (one atomic per warp) when the item changes and at the end
   double err_acc = 0.0;

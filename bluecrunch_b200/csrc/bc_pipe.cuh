@@ -182,6 +182,8 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB)
   }
   if (blockIdx.x < total) mid_tile_tw<TC, W, NT>(fac, tile_of(blockIdx.x), h);
   __syncthreads();
+  pdl_wait();
+  pdl_trigger();
   unsigned phases = 0;  // bit st: parity to wait for on bars[st]
   int st = 0;
   unsigned u = blockIdx.x;
@@ -253,6 +255,8 @@ __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_i
     fence_mbar_init();
   }
   __syncthreads();
+  pdl_wait();
+  pdl_trigger();
   unsigned phases = 0;  // bit st: parity to wait for on bars[st]
   int st = 0;
   unsigned u = blockIdx.x;
@@ -380,6 +384,8 @@ __device__ __forceinline__ void rows_load(double2 *dst, const CUtensorMap *map, 
 template <int L, bool SQ>
 __global__ void __launch_bounds__(RowTile<L>::NT, RowTile<L>::MINB)
     k2_rows(ClassParams p, const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB) {
+  pdl_wait();
+  pdl_trigger();
   using R = RowTile<L>;
   constexpr int TC = L / PTS, NR = R::NR, NS = R::SLOTS;
   extern __shared__ unsigned char smraw[];
@@ -519,6 +525,7 @@ template <int L> struct PackTile {
 
 template <int L>
 __global__ void __launch_bounds__(PassTile<L>::NT, PassTile<L>::MINB) k2_outer_fwd(ClassParams p) {
+  pdl_trigger();  // the first pass of a class: launched normally, lets the next one start early
   using T = PassTile<L>;
   using K = PackTile<L>;
   constexpr int W = T::W, TC = L / PTS, NT = T::NT;

@@ -150,6 +150,8 @@ __global__ void __launch_bounds__(32 * RW_WARPS, 2)
     fence_mbar_init();
   }
   __syncthreads();
+  pdl_wait();
+  pdl_trigger();
   const unsigned rows_item = p.M / RW_L;
   const unsigned total = (unsigned)p.nitems * rows_item;  // rows of the class, far below 2^32
   const FastDiv fd_rows(rows_item);
